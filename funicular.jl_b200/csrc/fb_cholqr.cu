@@ -1,0 +1,145 @@
+// cholqr2! (src/panelblas.jl:130-146) on a matrix resident in device memory.
+//
+// The reference runs each pass as gram -> host Cholesky -> rdiv_rows!, with
+// the k x k matrices crossing to the host and back twice per pass. Here the
+// whole chain is one fixed sequence of launches on one queue: every pass is
+// Gram (folded, Hermitian) -> single-CTA Cholesky with the shifted retry ->
+// row-parallel triangular solve, and the factors never leave the device. The
+// decisions the reference takes on the host are taken on the device through
+// a status block in the workspace: a pass whose Cholesky fails stops every
+// later kernel (Y keeps what the finished passes made of it, as when the
+// reference throws before its rdiv_rows!), and the third pass runs only if a
+// shift fired in pass 1 or 2.
+#include "fb_common.cuh"
+
+namespace fb {
+
+int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, int64_t ldb,
+                 int64_t rows, int kA, int kB, z64 alpha, z64 beta, bool hermitian,
+                 void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                 const ChainStatus* st, int gate);
+size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian);
+int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr,
+                 cudaStream_t stream, const ChainStatus* st, int gate);
+size_t potrf_gwork_bytes(int k);
+int potrf_enqueue(const z64* G, int64_t ldg, int k, int64_t N, z64* U, int64_t ldu,
+                  const z64* Rin, int64_t ldrin, z64* Rout, int64_t ldrout, z64* gwork,
+                  ChainStatus* st, int pass, int gate, cudaStream_t stream);
+
+struct CholqrLayout {
+    size_t status, G, U, Ra, Rb, gwork, gram, total;
+};
+
+static CholqrLayout cholqr_layout(int64_t N, int k) {
+    CholqrLayout L{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t at = off; off += align_up(bytes > 0 ? bytes : 1, 256); return at; };
+    const size_t kk = (size_t)k * k * sizeof(z64);
+    L.status = take(sizeof(ChainStatus));
+    L.G = take(kk);
+    L.U = take(kk);
+    L.Ra = take(kk);
+    L.Rb = take(kk);
+    L.gwork = take(potrf_gwork_bytes(k));
+    L.gram = take(gram_workspace_size(N, k, k, true));
+    L.total = off;
+    return L;
+}
+
+// Copies R of the last pass that ran into the caller's R.
+__global__ void select_r_kernel(z64* __restrict__ R, int64_t ldr, const z64* __restrict__ Ra,
+                                const z64* __restrict__ Rb, int k, const ChainStatus* st) {
+    if (st->failed) return;
+    const bool third = (st->shifted[1] | st->shifted[2]) != 0;
+    const z64* src = third ? Ra : Rb;
+    const int64_t kk = (int64_t)k * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < kk; e += (int64_t)gridDim.x * blockDim.x) {
+        int j = (int)(e / k), i = (int)(e - (int64_t)j * k);
+        R[i + (int64_t)j * ldr] = src[e];
+    }
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+int fb_zcholqr2_workspace_size(int64_t N, int k, size_t* bytes) {
+    if (!bytes || N < 0 || k < 0) { set_error(FB_EINVAL, "fb_zcholqr2_workspace_size: bad argument"); return FB_EINVAL; }
+    *bytes = cholqr_layout(N, k).total;
+    return FB_OK;
+}
+
+int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
+                void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    if (N < 1 || k < 1) {
+        set_error(FB_EINVAL, "cholqr2!: N and k must be positive, got N=%lld, k=%d", (long long)N, k);
+        return FB_EINVAL;
+    }
+    if (!Y || !R) { set_error(FB_EINVAL, "fb_zcholqr2: NULL matrix"); return FB_EINVAL; }
+    if (ldy < N || ldr < k) { set_error(FB_EDIM, "fb_zcholqr2: leading dimension too small"); return FB_EDIM; }
+    if (((uintptr_t)Y | (uintptr_t)R) & 15) {
+        set_error(FB_EINVAL, "fb_zcholqr2: device pointers must be 16-byte aligned");
+        return FB_EINVAL;
+    }
+    CholqrLayout L = cholqr_layout(N, k);
+    if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255)) {
+        set_error(FB_ENOMEM, "fb_zcholqr2: workspace must be 256-byte aligned and hold %zu bytes (got %zu)",
+                  L.total, workspace_bytes);
+        return FB_ENOMEM;
+    }
+    char* ws = static_cast<char*>(workspace);
+    ChainStatus* st = reinterpret_cast<ChainStatus*>(ws + L.status);
+    z64* G = reinterpret_cast<z64*>(ws + L.G);
+    z64* U = reinterpret_cast<z64*>(ws + L.U);
+    z64* Ra = reinterpret_cast<z64*>(ws + L.Ra);
+    z64* Rb = reinterpret_cast<z64*>(ws + L.Rb);
+    z64* gwork = reinterpret_cast<z64*>(ws + L.gwork);
+    void* gram_ws = ws + L.gram;
+    const size_t gram_bytes = L.total - L.gram;
+    cudaStream_t stream = stream_of(queue);
+    z64* Yz = reinterpret_cast<z64*>(Y);
+    const z64 one = zmake(1.0, 0.0), zero = zmake(0.0, 0.0);
+
+    FB_CUDA(cudaMemsetAsync(st, 0, sizeof(ChainStatus), stream), "cudaMemsetAsync");
+    // R accumulates as Ra = R1, Rb = R2 R1, Ra = R3 R2 R1.
+    const z64* rin[4] = {nullptr, nullptr, Ra, Rb};
+    z64* rout[4] = {nullptr, Ra, Rb, Ra};
+    for (int pass = 1; pass <= 3; ++pass) {
+        const int gate = pass == 3 ? GATE_THIRD : GATE_HEALTHY;
+        FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st, gate));
+        FB_TRY(potrf_enqueue(G, k, k, N, U, k, rin[pass], k, rout[pass], k, gwork, st, pass, gate, stream));
+        FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, stream, st, gate));
+    }
+    int blocks = (int)((int64_t)k * k + 255) / 256;
+    select_r_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<z64*>(R), ldr, Ra, Rb, k, st);
+    FB_LAUNCHED("select_r_kernel");
+
+    if (info) {
+        FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        return fb_zcholqr2_query(workspace, info, passes, nullptr);
+    }
+    return FB_OK;
+}
+
+int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shifts) {
+    if (!workspace) { set_error(FB_EINVAL, "fb_zcholqr2_query: NULL workspace"); return FB_EINVAL; }
+    ChainStatus host{};
+    FB_CUDA(cudaMemcpy(&host, workspace, sizeof host, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (info) *info = host.failed;
+    if (passes) *passes = (host.shifted[1] | host.shifted[2]) ? 3 : 2;
+    if (shifts)
+        for (int p = 0; p < 3; ++p) shifts[p] = host.shift[p + 1];
+    if (host.failed) {
+        set_error(FB_ENOTSPD,
+                  "the Gram matrix of pass %d is not positive definite even after a shift of %.17g, so the "
+                  "columns are numerically dependent: a zero column, a duplicated one, or a condition number "
+                  "past 4.5e15. Drop the dependent columns before orthonormalizing",
+                  host.failed, host.shift[host.failed]);
+        return FB_ENOTSPD;
+    }
+    return FB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+// The device API half of the backend: memory, page-locked slabs, queues,
+// events and pitched copies. Mirrors the contract of src/device_api.jl:5-138
+// as the reference's CUDA extension implements it
+// (ext/FunicularCUDAExt.jl:29-182), without any per-array stream bookkeeping:
+// ordering between queues is the caller's events alone.
+#include <cstdarg>
+#include <mutex>
+#include <vector>
+
+#include "fb_common.cuh"
+
+namespace fb {
+
+static thread_local std::string g_last_error;
+
+void set_error(int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    (void)status;
+    g_last_error = buf;
+}
+
+int cuda_status(cudaError_t err, const char* what) {
+    set_error(FB_ECUDA, "%s: %s (%s)", what, cudaGetErrorString(err), cudaGetErrorName(err));
+    return FB_ECUDA;
+}
+
+int sm_count() {
+    static std::mutex mu;
+    static std::vector<int> counts;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)counts.size() <= dev) counts.resize(dev + 1, 0);
+    if (counts[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        counts[dev] = n;
+    }
+    return counts[dev];
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+int fb_abi_version(void) { return FB_ABI_VERSION; }
+
+const char* fb_last_error(void) { return g_last_error.c_str(); }
+
+int fb_device_count(int* count) {
+    if (!count) { set_error(FB_EINVAL, "fb_device_count: count is NULL"); return FB_EINVAL; }
+    int n = 0;
+    cudaError_t err = cudaGetDeviceCount(&n);
+    if (err == cudaErrorNoDevice || err == cudaErrorInsufficientDriver) {
+        cudaGetLastError();
+        *count = 0;
+        return FB_OK;
+    }
+    FB_CUDA(err, "cudaGetDeviceCount");
+    *count = n;
+    return FB_OK;
+}
+
+int fb_set_device(int device) {
+    FB_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    return FB_OK;
+}
+
+int fb_alloc_device(void** ptr, size_t nbytes) {
+    if (!ptr) { set_error(FB_EINVAL, "fb_alloc_device: ptr is NULL"); return FB_EINVAL; }
+    *ptr = nullptr;
+    if (nbytes == 0) return FB_OK;
+    cudaError_t err = cudaMalloc(ptr, nbytes);
+    if (err == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        set_error(FB_ENOMEM, "fb_alloc_device: out of device memory allocating %zu bytes", nbytes);
+        return FB_ENOMEM;
+    }
+    FB_CUDA(err, "cudaMalloc");
+    // cudaMalloc is synchronous with respect to the device, so the buffer is
+    // ready for any stream on return, which is what alloc_device promises.
+    return FB_OK;
+}
+
+int fb_free_device(void* ptr) {
+    if (!ptr) return FB_OK;
+    FB_CUDA(cudaFree(ptr), "cudaFree");
+    return FB_OK;
+}
+
+int fb_alloc_host_slab(void** ptr, size_t nbytes) {
+    if (!ptr) { set_error(FB_EINVAL, "fb_alloc_host_slab: ptr is NULL"); return FB_EINVAL; }
+    *ptr = nullptr;
+    if (nbytes == 0) nbytes = 64;
+    cudaError_t err = cudaHostAlloc(ptr, nbytes, cudaHostAllocPortable);
+    if (err == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        set_error(FB_ENOMEM, "fb_alloc_host_slab: cannot page-lock %zu bytes of host memory", nbytes);
+        return FB_ENOMEM;
+    }
+    FB_CUDA(err, "cudaHostAlloc");
+    return FB_OK;
+}
+
+int fb_free_host_slab(void* ptr) {
+    if (!ptr) return FB_OK;
+    FB_CUDA(cudaFreeHost(ptr), "cudaFreeHost");
+    return FB_OK;
+}
+
+int fb_pin_host(void* ptr, size_t nbytes) {
+    if (!ptr || nbytes == 0) { set_error(FB_EINVAL, "fb_pin_host: empty range"); return FB_EINVAL; }
+    FB_CUDA(cudaHostRegister(ptr, nbytes, cudaHostRegisterPortable), "cudaHostRegister");
+    return FB_OK;
+}
+
+int fb_unpin_host(void* ptr) {
+    if (!ptr) return FB_OK;
+    FB_CUDA(cudaHostUnregister(ptr), "cudaHostUnregister");
+    return FB_OK;
+}
+
+int fb_queue_create(fb_queue_t* queue) {
+    if (!queue) { set_error(FB_EINVAL, "fb_queue_create: queue is NULL"); return FB_EINVAL; }
+    cudaStream_t s = nullptr;
+    FB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    *queue = reinterpret_cast<fb_queue_t>(s);
+    return FB_OK;
+}
+
+int fb_queue_destroy(fb_queue_t queue) {
+    if (!queue) return FB_OK;
+    FB_CUDA(cudaStreamDestroy(stream_of(queue)), "cudaStreamDestroy");
+    return FB_OK;
+}
+
+int fb_event_record(fb_queue_t queue, fb_event_t* event) {
+    if (!event) { set_error(FB_EINVAL, "fb_event_record: event is NULL"); return FB_EINVAL; }
+    cudaEvent_t e = nullptr;
+    FB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreateWithFlags");
+    cudaError_t err = cudaEventRecord(e, stream_of(queue));
+    if (err != cudaSuccess) {
+        cudaEventDestroy(e);
+        return cuda_status(err, "cudaEventRecord");
+    }
+    *event = reinterpret_cast<fb_event_t>(e);
+    return FB_OK;
+}
+
+int fb_event_destroy(fb_event_t event) {
+    if (!event) return FB_OK;
+    FB_CUDA(cudaEventDestroy(reinterpret_cast<cudaEvent_t>(event)), "cudaEventDestroy");
+    return FB_OK;
+}
+
+int fb_queue_wait_event(fb_queue_t queue, fb_event_t event) {
+    if (!event) return FB_OK;
+    FB_CUDA(cudaStreamWaitEvent(stream_of(queue), reinterpret_cast<cudaEvent_t>(event), 0),
+            "cudaStreamWaitEvent");
+    return FB_OK;
+}
+
+int fb_queue_sync(fb_queue_t queue) {
+    FB_CUDA(cudaStreamSynchronize(stream_of(queue)), "cudaStreamSynchronize");
+    return FB_OK;
+}
+
+int fb_event_sync(fb_event_t event) {
+    if (!event) return FB_OK;
+    FB_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(event)), "cudaEventSynchronize");
+    return FB_OK;
+}
+
+int fb_event_query(fb_event_t event, int* done) {
+    if (!done) { set_error(FB_EINVAL, "fb_event_query: done is NULL"); return FB_EINVAL; }
+    if (!event) { *done = 1; return FB_OK; }
+    cudaError_t err = cudaEventQuery(reinterpret_cast<cudaEvent_t>(event));
+    if (err == cudaErrorNotReady) {
+        cudaGetLastError();
+        *done = 0;
+        return FB_OK;
+    }
+    FB_CUDA(err, "cudaEventQuery");
+    *done = 1;
+    return FB_OK;
+}
+
+int fb_sync_all(void) {
+    FB_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    return FB_OK;
+}
+
+int fb_copy2d(void* dst, size_t dpitch, const void* src, size_t spitch,
+              size_t width_bytes, size_t cols, fb_queue_t queue) {
+    if (width_bytes == 0 || cols == 0) return FB_OK;
+    if (!dst || !src) { set_error(FB_EINVAL, "fb_copy2d: NULL pointer"); return FB_EINVAL; }
+    if (dpitch < width_bytes || spitch < width_bytes) {
+        set_error(FB_EINVAL, "fb_copy2d: a pitch (%zu, %zu) is narrower than a column of %zu bytes",
+                  dpitch, spitch, width_bytes);
+        return FB_EINVAL;
+    }
+    if (queue == nullptr) {
+        FB_CUDA(cudaMemcpy2D(dst, dpitch, src, spitch, width_bytes, cols, cudaMemcpyDefault), "cudaMemcpy2D");
+        return FB_OK;
+    }
+    FB_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width_bytes, cols, cudaMemcpyDefault, stream_of(queue)),
+            "cudaMemcpy2DAsync");
+    return FB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+"""The kernel overrides of the B200 backend: the four functions of
+src/kernels.jl that a vendor backend specialises (the pattern of
+ext/FunicularMetalExt.jl:187-189), plus the device hooks the reference does
+not have yet: the k x k Cholesky with its shifted retry (cholesky_upper,
+src/panelblas.jl:148-155) and the whole device-resident cholqr2!.
+
+Every function checks shapes the way the reference does (DimensionMismatch)
+before anything reaches the device, then makes one C call whose kernels land on
+the backend's current queue (the one `submit` set), or on the default stream
+outside a sweep.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import ArgumentError, DimensionMismatch, NotPositiveDefinite, call, z128
+from .device_api import DeviceMatrix, eltype_code
+
+EPS64 = float(np.finfo(np.float64).eps)
+
+
+def _vp(x):
+    return ctypes.c_void_p(x)
+
+
+def _need_complex128(*mats):
+    for m in mats:
+        if not isinstance(m, DeviceMatrix):
+            raise ArgumentError(f"the B200 kernels take device matrices, got {type(m).__name__}")
+        if m.dtype != np.complex128:
+            raise ArgumentError(f"the B200 kernels compute in ComplexF64, got {m.dtype}")
+
+
+def convert_copy(backend, dst: DeviceMatrix, src: DeviceMatrix) -> DeviceMatrix:
+    """convert_copy! (src/kernels.jl:14-20)."""
+    if tuple(dst.shape) != tuple(src.shape):
+        raise DimensionMismatch(f"copy between a {tuple(dst.shape)} destination and a {tuple(src.shape)} source")
+    if dst.size == 0:
+        return dst
+    call("fb_convert_copy", _vp(dst.ptr), eltype_code(dst.dtype), ctypes.c_int64(dst.ld),
+         _vp(src.ptr), eltype_code(src.dtype), ctypes.c_int64(src.ld),
+         ctypes.c_int64(dst.rows), ctypes.c_int64(dst.cols), backend.queue_handle())
+    return dst
+
+
+def gram_accumulate(backend, C: DeviceMatrix, A: DeviceMatrix, B: DeviceMatrix, alpha, beta) -> DeviceMatrix:
+    """gram_accumulate! (src/kernels.jl:40): C <- alpha A^H B + beta C, with
+    beta == 0 overwriting whatever C held."""
+    _need_complex128(C, A, B)
+    if not (A.rows == B.rows and tuple(C.shape) == (A.cols, B.cols)):
+        raise DimensionMismatch(f"cannot accumulate the {A.shape}' times {B.shape} product into a {C.shape} matrix")
+    if C.size == 0:
+        return C
+    lib = _lib.load()
+    hermitian = 1 if A.same_view(B) else 0
+    need = ctypes.c_size_t(0)
+    call("fb_zgram_workspace_size", ctypes.c_int64(A.rows), A.cols, B.cols, hermitian, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    try:
+        status = lib.fb_zgram(_vp(C.ptr), C.ld, _vp(A.ptr), max(A.ld, 1), _vp(B.ptr), max(B.ld, 1),
+                              A.rows, A.cols, B.cols, z128(alpha), z128(beta), _vp(ws), ws_bytes,
+                              backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    _lib.check(status, "gram_accumulate!")
+    return C
+
+
+def rdiv_upper(backend, Y: DeviceMatrix, R: DeviceMatrix) -> DeviceMatrix:
+    """rdiv_upper! (src/kernels.jl:108): Y <- Y R^-1, R upper triangular."""
+    _need_complex128(Y, R)
+    if not (R.rows == R.cols == Y.cols):
+        raise DimensionMismatch(f"a {Y.shape} block cannot be divided by a {R.shape} triangular factor")
+    if Y.size == 0:
+        return Y
+    call("fb_ztrsm_right_upper", _vp(Y.ptr), ctypes.c_int64(Y.ld), ctypes.c_int64(Y.rows), Y.cols,
+         _vp(R.ptr), ctypes.c_int64(R.ld), backend.queue_handle())
+    return Y
+
+
+def rightmul_gemm(backend, dst: DeviceMatrix, A: DeviceMatrix, C: DeviceMatrix) -> DeviceMatrix:
+    """rightmul_gemm! (src/kernels.jl:73): dst <- A C."""
+    _need_complex128(dst, A, C)
+    if not (A.cols == C.rows and tuple(dst.shape) == (A.rows, C.cols)):
+        raise DimensionMismatch(f"cannot multiply a {A.shape} block by a {C.shape} factor into a {dst.shape} matrix")
+    if dst.size == 0:
+        return dst
+    call("fb_zgemm_right", _vp(dst.ptr), ctypes.c_int64(dst.ld), _vp(A.ptr), ctypes.c_int64(max(A.ld, 1)),
+         ctypes.c_int64(A.rows), A.cols, _vp(C.ptr), ctypes.c_int64(max(C.ld, 1)), C.cols, backend.queue_handle())
+    return dst
+
+
+def cholesky_upper_device(backend, G: DeviceMatrix, N: int, k: int, U: DeviceMatrix,
+                          Rin: DeviceMatrix | None = None, Rout: DeviceMatrix | None = None):
+    """cholesky_upper(G, N, k) (src/panelblas.jl:148-155) on the device. Writes
+    U; with Rin, also Rout = U Rin. Returns (shifted, shift). Waits for the
+    queue, since the caller branches on `shifted`."""
+    _need_complex128(G, U)
+    if G.shape != (k, k) or U.shape != (k, k):
+        raise DimensionMismatch(f"cholesky_upper: a {k}x{k} factor of a {G.shape} matrix into {U.shape}")
+    need = ctypes.c_size_t(0)
+    call("fb_zpotrf_workspace_size", k, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    shifted = ctypes.c_int(0)
+    shift = ctypes.c_double(0.0)
+    lib = _lib.load()
+    try:
+        status = lib.fb_zpotrf_shifted(
+            _vp(U.ptr), U.ld, _vp(G.ptr), G.ld, k, N,
+            _vp(Rin.ptr if Rin is not None else None), Rin.ld if Rin is not None else k,
+            _vp(Rout.ptr if Rout is not None else None), Rout.ld if Rout is not None else k,
+            ctypes.byref(shifted), ctypes.byref(shift), _vp(ws), ws_bytes, backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    if status == _lib.FB_ENOTSPD:
+        raise NotPositiveDefinite(_lib.last_error())
+    _lib.check(status, "cholesky_upper")
+    return bool(shifted.value), float(shift.value)
+
+
+def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True):
+    """cholqr2! (src/panelblas.jl:130-139) on a matrix already in device
+    memory: Y becomes Q in place and R (k x k) is written. With wait=True the
+    call returns (passes, shifts) and raises if a Gram matrix stayed
+    indefinite; with wait=False it only enqueues."""
+    _need_complex128(Y, R)
+    N, k = Y.shape
+    if R.shape != (k, k):
+        raise DimensionMismatch(f"cholqr2! of an {N}x{k} matrix writes a {k}x{k} R, got {R.shape}")
+    need = ctypes.c_size_t(0)
+    call("fb_zcholqr2_workspace_size", ctypes.c_int64(N), k, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    lib = _lib.load()
+    info = ctypes.c_int(0)
+    passes = ctypes.c_int(0)
+    try:
+        status = lib.fb_zcholqr2(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld,
+                                 ctypes.byref(info) if wait else None, ctypes.byref(passes) if wait else None,
+                                 _vp(ws), ws_bytes, backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    if not wait:
+        _lib.check(status, "cholqr2!")
+        return None
+    shifts = (ctypes.c_double * 3)()
+    if status == _lib.FB_OK:
+        status = lib.fb_zcholqr2_query(_vp(ws), None, None, shifts)
+    if status == _lib.FB_ENOTSPD:
+        raise NotPositiveDefinite(_lib.last_error())
+    _lib.check(status, "cholqr2!")
+    return passes.value, tuple(shifts)

@@ -1,0 +1,183 @@
+/*
+ * libfunicular_b200 — C ABI of the B200 device backend for Funicular's panel
+ * linear algebra.
+ *
+ * Every entry point takes plain pointers, sizes and opaque queue handles, and
+ * returns an int status (FB_OK = 0). A non-zero status leaves a message that
+ * fb_last_error() returns on the same host thread. The statuses map onto the
+ * exceptions the reference raises:
+ *   FB_EINVAL  -> ArgumentError      FB_EDIM   -> DimensionMismatch
+ *   FB_ENOTSPD -> ArgumentError (the Gram matrix is not positive definite even
+ *                 after the shift, src/panelblas.jl:153)
+ *
+ * Matrices are column major ComplexF64 (16 bytes, re then im), the first
+ * dimension contiguous, with a leading dimension in elements, exactly the
+ * layout Funicular's panels and staging buffers have
+ * (ext/FunicularCUDAExt.jl:154-163). Device pointers must be 16-byte aligned.
+ *
+ * A queue is a non-blocking CUDA stream (fb_queue_t). Passing NULL as a
+ * queue means "complete on return" for copies (the reference's queue=nothing)
+ * and the legacy per-thread default stream for kernels. Kernels never
+ * synchronize the host unless their comment says so.
+ *
+ * Citations name the reference function each entry point replaces, as
+ * file:line within Funicular.jl.
+ */
+#ifndef FUNICULAR_B200_H
+#define FUNICULAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FB_ABI_VERSION 1
+
+enum fb_status_code {
+    FB_OK = 0,
+    FB_EINVAL = 1,    /* bad argument: ArgumentError */
+    FB_EDIM = 2,      /* shape mismatch: DimensionMismatch */
+    FB_ENOMEM = 3,    /* allocation failed or workspace too small */
+    FB_ENOTSPD = 4,   /* not positive definite even after the shift */
+    FB_ECUDA = 5,     /* the CUDA runtime reported an error */
+    FB_ENOTSUP = 6    /* shape or type this build does not handle */
+};
+
+/* Element types for fb_convert_copy (ComplexF64, ComplexF32, Float64, Float32). */
+enum fb_eltype { FB_C128 = 0, FB_C64 = 1, FB_F64 = 2, FB_F32 = 3 };
+
+typedef struct { double re, im; } fb_z128;
+typedef void* fb_queue_t;
+typedef void* fb_event_t;
+
+/* ---- library ---------------------------------------------------------- */
+
+int fb_abi_version(void);
+/* The message of the last failing call on this host thread ("" if none). */
+const char* fb_last_error(void);
+/* Number of visible CUDA devices (0 on a machine without a GPU). */
+int fb_device_count(int* count);
+int fb_set_device(int device);
+
+/* ---- device API: src/device_api.jl:5-138, ext/FunicularCUDAExt.jl ------ */
+
+/* alloc_device(backend, T, dims) (src/device_api.jl:19,
+ * ext/FunicularCUDAExt.jl:32-40). Complete on return. */
+int fb_alloc_device(void** ptr, size_t nbytes);
+int fb_free_device(void* ptr);
+
+/* alloc_host_slab(backend, nbytes) (src/device_api.jl:28,
+ * ext/FunicularCUDAExt.jl:45-49): page-locked host memory, so that copies
+ * out of it are asynchronous. The pointer is at least 64-byte aligned
+ * (SLAB_ALIGN, src/device_api.jl:140). */
+int fb_alloc_host_slab(void** ptr, size_t nbytes);
+int fb_free_host_slab(void* ptr);
+/* Page-locks host memory the caller already owns (CUDA.pin in the
+ * reference's CUDA backend). */
+int fb_pin_host(void* ptr, size_t nbytes);
+int fb_unpin_host(void* ptr);
+
+/* make_queue(backend) (src/device_api.jl:53, ext/FunicularCUDAExt.jl:73-76):
+ * a non-blocking stream, so it never serializes against the legacy default
+ * stream. */
+int fb_queue_create(fb_queue_t* queue);
+int fb_queue_destroy(fb_queue_t queue);
+/* record_event(backend, queue) (src/device_api.jl:81,
+ * ext/FunicularCUDAExt.jl:91-95): a new timing-free event recorded on queue. */
+int fb_event_record(fb_queue_t queue, fb_event_t* event);
+int fb_event_destroy(fb_event_t event);
+/* wait_event(backend, queue, event) (src/device_api.jl:88,
+ * ext/FunicularCUDAExt.jl:99-102): a device-side wait, the host carries on. */
+int fb_queue_wait_event(fb_queue_t queue, fb_event_t event);
+/* sync_queue / sync_event / sync_all (src/device_api.jl:95,102,109). A
+ * failure of earlier work on the queue surfaces here as FB_ECUDA. */
+int fb_queue_sync(fb_queue_t queue);
+int fb_event_sync(fb_event_t event);
+/* *done = 1 once the event has been signalled. */
+int fb_event_query(fb_event_t event, int* done);
+int fb_sync_all(void);
+
+/* h2d!/d2h! and device-to-device copies (src/device_api.jl:37,45;
+ * copy_region! at ext/FunicularCUDAExt.jl:138-152): a 2-D copy of `cols`
+ * columns of `width_bytes` each, the columns `dpitch`/`spitch` bytes apart.
+ * Covers a whole panel, a column range of a staging buffer and a row block
+ * slice of a panel. queue == NULL: complete on return; otherwise enqueued. */
+int fb_copy2d(void* dst, size_t dpitch, const void* src, size_t spitch,
+              size_t width_bytes, size_t cols, fb_queue_t queue);
+
+/* ---- kernels: src/kernels.jl ----------------------------------------- */
+
+/* convert_copy!(backend, dst, src) (src/kernels.jl:14): elementwise
+ * conversion between two rows x cols device views with leading dimensions
+ * ldd and lds (in elements of their own type). Complex to real is refused. */
+int fb_convert_copy(void* dst, int dst_type, int64_t ldd,
+                    const void* src, int src_type, int64_t lds,
+                    int64_t rows, int64_t cols, fb_queue_t queue);
+
+/* gram_accumulate!(backend, C, A, B, alpha, beta) (src/kernels.jl:40):
+ * C <- alpha * A^H B + beta * C with A rows x kA, B rows x kB, C kA x kB.
+ * beta == 0 overwrites C without reading it (a pooled buffer may hold NaN,
+ * src/kernels.jl:29-30). When A and B are the same view (same pointer, ld and
+ * width) only the upper triangle is computed and the lower one is its
+ * conjugate mirror, so the result is Hermitian to the bit. The reduction
+ * order depends only on rows, kA, kB and the device, never on the caller's
+ * pipelining, so repeated calls give identical bits.
+ * workspace must hold fb_zgram_workspace_size bytes of device memory. */
+int fb_zgram_workspace_size(int64_t rows, int kA, int kB, int hermitian, size_t* bytes);
+int fb_zgram(fb_z128* C, int64_t ldc,
+             const fb_z128* A, int64_t lda, const fb_z128* B, int64_t ldb,
+             int64_t rows, int kA, int kB, fb_z128 alpha, fb_z128 beta,
+             void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* rdiv_upper!(backend, Y, R) (src/kernels.jl:108): Y <- Y R^-1 in place for
+ * an upper triangular, non-unit k x k R; Y is rows x k with leading
+ * dimension ldy (a row block view of a staging buffer is fine). */
+int fb_ztrsm_right_upper(fb_z128* Y, int64_t ldy, int64_t rows, int k,
+                         const fb_z128* R, int64_t ldr, fb_queue_t queue);
+
+/* rightmul_gemm!(backend, dst, A, C) (src/kernels.jl:73): dst <- A C with A
+ * rows x s, C s x r, dst rows x r. dst must not overlap A. */
+int fb_zgemm_right(fb_z128* dst, int64_t ldd, const fb_z128* A, int64_t lda,
+                   int64_t rows, int s, const fb_z128* C, int64_t ldc, int r,
+                   fb_queue_t queue);
+
+/* cholesky_upper(G, N, k) (src/panelblas.jl:148-155) on the device: U upper
+ * with U^H U = G, reading G's upper triangle. When G is not positive
+ * definite it factors G + s I with s = 11 N k eps(Float64) ||G||_F instead.
+ * If Rin is non-NULL, Rout <- U * Rin (the R2 * R product of
+ * src/panelblas.jl:133,136); Rout must not alias Rin. U and Rout are written
+ * in full, zeros below the diagonal. Synchronizes `queue` and reports:
+ * *shifted = 1 if the shift was taken, *shift = s. Returns FB_ENOTSPD when
+ * even G + s I fails. workspace: fb_zpotrf_workspace_size bytes. */
+int fb_zpotrf_workspace_size(int k, size_t* bytes);
+int fb_zpotrf_shifted(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg,
+                      int k, int64_t N, const fb_z128* Rin, int64_t ldrin,
+                      fb_z128* Rout, int64_t ldrout,
+                      int* shifted, double* shift,
+                      void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* cholqr2!(Y) (src/panelblas.jl:130-146) on a device-resident matrix: two
+ * passes of gram -> cholesky_upper -> rdiv_rows!, a third pass when either
+ * shifted, R = R3 R2 R1 written to R (k x k, zeros below the diagonal).
+ * Every step runs on `queue`; the branch to the third pass and the stop after
+ * a failed factorization are taken on the device, so the call enqueues a
+ * fixed sequence of launches. With info != NULL the call synchronizes and
+ * sets *info = 0, or the 1-based pass whose Gram was not positive definite
+ * (returning FB_ENOTSPD); *passes = 2 or 3 if non-NULL. With info == NULL it
+ * returns at once and fb_zcholqr2_query reads the outcome after the queue
+ * has drained. workspace: fb_zcholqr2_workspace_size bytes, 256-byte
+ * aligned; the same workspace must not be used by two calls in flight. */
+int fb_zcholqr2_workspace_size(int64_t N, int k, size_t* bytes);
+int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
+                fb_z128* R, int64_t ldr, int* info, int* passes,
+                void* workspace, size_t workspace_bytes, fb_queue_t queue);
+int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
+                      double* shifts /* 3 entries, or NULL */);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FUNICULAR_B200_H */

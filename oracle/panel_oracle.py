@@ -1,0 +1,225 @@
+"""CPU oracle for the panel linear algebra hot path.
+
+TEST INFRASTRUCTURE ONLY. This module restates, in numpy and scipy's LAPACK,
+what Funicular.jl's CPU reference backend computes for the functions on the
+hot path, step for step in the reference's order. Only tests/, the smoke check
+in __graft_entry__.py and bench.py's CPU-baseline leg may import it, and only
+to check or time the reference's algorithm; the B200 backend never calls it.
+
+Where the reference's arithmetic lives:
+  * its own code: row-block traversal, the accumulation rule of gram, the pass
+    structure and shift rule of cholqr2!, the step order of project. These
+    are restated below, each function citing the lines it follows.
+  * Julia's LinearAlgebra, which calls OpenBLAS and LAPACK (zgemm, ztrsm,
+    zpotrf). No Manifest pins a version (Project.toml:34 asks for julia 1.10).
+    The stand-in here is the OpenBLAS/LAPACK that scipy bundles; both are
+    reference-LAPACK zpotrf/ztrsm semantics.
+
+Parity pin. The reference publishes no golden vectors for this path; its own
+tests check it against dense LinearAlgebra within blastol = 100 eps sqrt(N k)
+and orthogonality_bound = 100 N k eps (test/setup.jl:170-172), and check
+several results for bitwise equality. tests/test_oracle.py restates those
+known-answer tests against this oracle, which is how the oracle is pinned.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import scipy.linalg.blas as blas
+import scipy.linalg.lapack as lapack
+
+EPS = {np.dtype(np.complex128): 2.0 ** -52, np.dtype(np.float64): 2.0 ** -52,
+       np.dtype(np.complex64): 2.0 ** -23, np.dtype(np.float32): 2.0 ** -23}
+
+
+class OracleArgumentError(ValueError):
+    pass
+
+
+# ---- plan arithmetic: src/plan.jl ------------------------------------------
+
+def row_block_height(N: int, k: int, w: int) -> int:
+    """row_block_height (src/plan.jl:133)."""
+    return max(1, min(N, (N * w) // k))
+
+
+def row_steps(N: int, height: int):
+    """RowSteps(N, height) (src/executor.jl:33-36): unit ranges as (start, stop)."""
+    h = max(1, min(int(height), int(N)))
+    return [(top, min(top + h, N)) for top in range(0, N, h)]
+
+
+def row_blocks(N: int, k: int, w: int):
+    """rowtraversal (src/executor.jl:38)."""
+    return row_steps(N, row_block_height(N, k, w))
+
+
+def panel_ranges(k: int, w: int):
+    """Column ranges of the panels of an N x k matrix cut at width w
+    (src/panels.jl:66-69): ragged last panel."""
+    return [(j * w, min((j + 1) * w, k)) for j in range((k + w - 1) // w)]
+
+
+def choose_panel_width(N, k, itemsize, device_budget, nbuffers=2, extra_buffers=0,
+                       workspace_bytes=0, target_panel_bytes=2 * 1024 ** 3):
+    """choose_panel_width (src/plan.jl:112-123)."""
+    if N <= 0:
+        raise OracleArgumentError(f"N must be positive, got {N}")
+    if k <= 0:
+        raise OracleArgumentError(f"k must be positive, got {k}")
+    buffers = nbuffers + extra_buffers
+    if buffers < 1:
+        raise OracleArgumentError("nbuffers + extra_buffers must be at least 1")
+    column = N * itemsize
+    available = int(math.floor(device_budget)) - int(math.floor(workspace_bytes))
+    per_buffer = available // buffers
+    if per_buffer < column:
+        raise OracleArgumentError("device budget too small for one column")
+    w = min(k, max(1, min(int(math.floor(target_panel_bytes)), per_buffer) // column))
+    npanels = -(-k // w)
+    return -(-k // npanels)
+
+
+# ---- kernels: src/kernels.jl ------------------------------------------------
+
+def gram_accumulate(C, A, B, alpha, beta):
+    """gram_accumulate! (src/kernels.jl:22-55): C <- alpha A^H B + beta C, a
+    zero beta overwriting C (NaN-safe)."""
+    prod = A.conj().T @ B
+    if beta == 0:
+        C[...] = alpha * prod
+    else:
+        C[...] = alpha * prod + beta * C
+    return C
+
+
+def rdiv_upper(Y, R):
+    """rdiv_upper! (src/kernels.jl:90-124) as rdiv!(Y, UpperTriangular(R)),
+    which LinearAlgebra sends to BLAS ztrsm (Right, Upper, NoTrans, NonUnit)."""
+    if Y.size == 0:
+        return Y
+    trsm = blas.ztrsm if np.iscomplexobj(Y) else blas.dtrsm
+    Y[...] = trsm(1.0, np.asfortranarray(R), np.asfortranarray(Y), side=1, lower=0, trans_a=0, diag=0)
+    return Y
+
+
+def rightmul_gemm(dst, A, C):
+    """rightmul_gemm! (src/kernels.jl:57-88)."""
+    dst[...] = A @ C
+    return dst
+
+
+# ---- panel BLAS: src/panelblas.jl --------------------------------------------
+
+def gram(X, Y=None, w=None):
+    """gram(X[, Y]) (src/panelblas.jl:33-53): C = X^H Y accumulated one row
+    block at a time, the first block overwriting (carry, :59)."""
+    N, k = X.shape
+    w = k if w is None else w
+    same = Y is None or Y is X
+    Y = X if Y is None else Y
+    C = np.empty((k, Y.shape[1]), dtype=X.dtype)
+    for step, (r0, r1) in enumerate(row_blocks(N, k, w)):
+        Xb = X[r0:r1]
+        Yb = Xb if same else Y[r0:r1]
+        gram_accumulate(C, Xb, Yb, 1.0, 0.0 if step == 0 else 1.0)
+    return C
+
+
+def cholesky_upper(G, N, k):
+    """cholesky_upper (src/panelblas.jl:148-155): zpotrf on the upper
+    triangle; on failure factor G + s I with s = 11 N k eps ||G||_F, and raise
+    if that fails too. Returns (U, shifted)."""
+    potrf = lapack.zpotrf if np.iscomplexobj(G) else lapack.dpotrf
+    U, info = potrf(np.asfortranarray(G), lower=0, clean=1)
+    if info == 0:
+        return np.triu(U), False
+    eps = EPS[np.dtype(G.dtype)]
+    shift = 11 * N * k * eps * np.linalg.norm(G)
+    U, info = potrf(np.asfortranarray(G + shift * np.eye(k)), lower=0, clean=1)
+    if info != 0:
+        raise OracleArgumentError(
+            f"the {k}x{k} Gram matrix is not positive definite even after a shift of {shift}")
+    return np.triu(U), True
+
+
+def rdiv_rows(Y, R, w=None):
+    """rdiv_rows! (src/panelblas.jl:157-169): Y <- Y R^-1 one row block at a
+    time."""
+    N, k = Y.shape
+    w = k if w is None else w
+    for r0, r1 in row_blocks(N, k, w):
+        rdiv_upper(Y[r0:r1], R)
+    return Y
+
+
+def cholqr_pass(Y, w=None):
+    """cholqr_pass! (src/panelblas.jl:141-146)."""
+    N, k = Y.shape
+    G = gram(Y, w=w)
+    R, shifted = cholesky_upper(G, N, k)
+    rdiv_rows(Y, R, w)
+    return R, shifted
+
+
+def cholqr2(Y, w=None):
+    """cholqr2! (src/panelblas.jl:130-139): two passes, a third if either
+    shifted, R = R2 R1 (R3 R2 R1). Y is overwritten with Q. Returns
+    (R, passes)."""
+    R, s1 = cholqr_pass(Y, w)
+    R2, s2 = cholqr_pass(Y, w)
+    R = R2 @ R
+    passes = 2
+    if s1 or s2:
+        R3, _ = cholqr_pass(Y, w)
+        R = R3 @ R
+        passes = 3
+    return R, passes
+
+
+def panelmul(G, X, w=None):
+    """panelmul!(Y, G, X) (src/panelblas.jl:91-100): Y[:, panel] = G X[:, panel]."""
+    k = X.shape[1]
+    w = k if w is None else w
+    Y = np.empty((G.shape[0], k), dtype=X.dtype)
+    for c0, c1 in panel_ranges(k, w):
+        Y[:, c0:c1] = G @ X[:, c0:c1]
+    return Y
+
+
+def project(Q, G, w=None):
+    """project(Q, G) (src/panelblas.jl:268-301): for each panel j, apply G to
+    Q_j, then fill block column j with Q_i^H (G Q_j) for every panel i."""
+    N, k = Q.shape
+    w = k if w is None else w
+    S = np.empty((k, k), dtype=Q.dtype)
+    ranges = panel_ranges(k, w)
+    for (c0, c1) in ranges:
+        image = G @ Q[:, c0:c1]
+        for (r0, r1) in ranges:
+            gram_accumulate(S[r0:r1, c0:c1], Q[:, r0:r1], image, 1.0, 0.0)
+    return S
+
+
+# ---- error measures the north star reports ------------------------------------
+
+def orthogonality_error(Q):
+    """||Q^H Q - I||_F."""
+    k = Q.shape[1]
+    return float(np.linalg.norm(Q.conj().T @ Q - np.eye(k)))
+
+
+def reconstruction_error(Y, Q, R):
+    """||Y - Q R|| / ||Y|| (Frobenius)."""
+    return float(np.linalg.norm(Y - Q @ R) / np.linalg.norm(Y))
+
+
+def blastol(dtype, N, k):
+    """test/setup.jl:170."""
+    return 100 * EPS[np.dtype(dtype)] * math.sqrt(N * k)
+
+
+def orthogonality_bound(dtype, N, k):
+    """test/setup.jl:172."""
+    return 100 * N * k * EPS[np.dtype(dtype)]

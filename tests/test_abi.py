@@ -1,0 +1,111 @@
+"""The C ABI: the library loads on a machine without a GPU, exports every
+function its header declares, and turns bad arguments into the statuses the
+reference's exceptions map onto, before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "funicular_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_device_api_and_kernels():
+    names = declared_functions()
+    for required in ("fb_alloc_device", "fb_alloc_host_slab", "fb_queue_create", "fb_event_record",
+                     "fb_queue_wait_event", "fb_queue_sync", "fb_event_sync", "fb_sync_all", "fb_copy2d",
+                     "fb_convert_copy", "fb_zgram", "fb_ztrsm_right_upper", "fb_zgemm_right",
+                     "fb_zpotrf_shifted", "fb_zcholqr2"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(fb):
+    lib = fb._lib.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), f"{name} is declared in the header but not exported"
+        assert name in fb._lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_binding_declares_nothing_the_header_lacks(fb):
+    assert set(fb._lib.SIGNATURES) <= set(declared_functions())
+
+
+def test_abi_version(fb):
+    assert fb._lib.load().fb_abi_version() == 1
+
+
+def test_device_count_without_a_gpu_is_not_an_error(fb):
+    assert fb._lib.device_count() >= 0
+
+
+def test_shape_errors_map_to_dimension_mismatch(fb):
+    lib = fb._lib.load()
+    z = fb._lib.z128(1.0)
+    status = lib.fb_zgram(None, 1, None, 1, None, 1, -1, 2, 2, z, z, None, 0, None)
+    assert status == fb._lib.FB_EDIM
+    assert "negative" in fb._lib.last_error()
+    with pytest.raises(fb.DimensionMismatch):
+        fb._lib.check(status)
+    assert lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None) == fb._lib.FB_EDIM
+    assert lib.fb_zgemm_right(None, 1, None, 1, 4, -1, None, 1, 2, None) == fb._lib.FB_EDIM
+
+
+def test_leading_dimension_is_checked(fb):
+    lib = fb._lib.load()
+    z = fb._lib.z128(1.0)
+    fake = ctypes.c_void_p(1 << 20)
+    status = lib.fb_zgram(fake, 4, fake, 3, fake, 8, 8, 4, 4, z, z, fake, 1 << 20, None)
+    assert status == fb._lib.FB_EDIM
+    assert "leading dimension" in fb._lib.last_error()
+
+
+def test_empty_work_is_a_no_op(fb):
+    lib = fb._lib.load()
+    z = fb._lib.z128(1.0)
+    assert lib.fb_zgram(None, 1, None, 1, None, 1, 10, 0, 3, z, z, None, 0, None) == fb._lib.FB_OK
+    assert lib.fb_ztrsm_right_upper(None, 1, 0, 3, None, 1, None) == fb._lib.FB_OK
+    assert lib.fb_copy2d(None, 16, None, 16, 0, 4, None) == fb._lib.FB_OK
+
+
+def test_workspace_queries(fb):
+    lib = fb._lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.fb_zpotrf_workspace_size(64, ctypes.byref(n)) == fb._lib.FB_OK and n.value > 0
+    assert lib.fb_zgram_workspace_size(100, 4, 5, 1, ctypes.byref(n)) == fb._lib.FB_EDIM
+    assert lib.fb_zcholqr2_workspace_size(-1, 4, ctypes.byref(n)) == fb._lib.FB_EINVAL
+
+
+def test_bad_eltype_and_complex_to_real_are_refused(fb):
+    lib = fb._lib.load()
+    fake = ctypes.c_void_p(1 << 20)
+    assert lib.fb_convert_copy(fake, 9, 4, fake, 0, 4, 4, 4, None) == fb._lib.FB_EINVAL
+    assert lib.fb_convert_copy(fake, fb._lib.FB_F64, 4, fake, fb._lib.FB_C128, 4, 4, 4, None) == fb._lib.FB_EINVAL
+    assert "complex" in fb._lib.last_error()
+
+
+def test_cholqr2_rejects_empty_and_misaligned(fb):
+    lib = fb._lib.load()
+    assert lib.fb_zcholqr2(None, 1, 0, 4, None, 4, None, None, None, 0, None) == fb._lib.FB_EINVAL
+    odd = ctypes.c_void_p((1 << 20) + 8)
+    assert lib.fb_zcholqr2(odd, 8, 8, 4, odd, 4, None, None, None, 0, None) == fb._lib.FB_EINVAL
+    assert "aligned" in fb._lib.last_error()
+
+
+def test_errors_are_per_thread(fb):
+    import threading
+    lib = fb._lib.load()
+    lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None)
+    seen = []
+    t = threading.Thread(target=lambda: seen.append(fb._lib.last_error()))
+    t.start()
+    t.join()
+    assert seen == [""]
+    assert fb._lib.last_error() != ""

@@ -1,0 +1,468 @@
+#!/usr/bin/env python
+"""cholqr2! throughput on the B200 backend.
+
+Workload (one step): cholqr2! of a device-resident ComplexF64 matrix with
+N = 10^7 rows and k = 64 columns (panel width 16, so the reference's row
+blocks are 2.5e6 rows), Y = U diag(s) V^H with U a seeded complex Gaussian made
+orthonormal, V a seeded 64 x 64 Haar unitary and s log-spaced from 1 to 1e-6.
+The metric is GB/s of algorithmic traffic, 96 N k bytes per cholqr2! (two
+passes of Gram read + TRSM read + TRSM write), over the device time of the
+step; the inputs (10.24 GB) are larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N under torchrun every rank runs its own replica (one matrix per
+GPU, no collective on the data path) and `value` is the bytes of all ranks over
+the slowest rank's time. --impl reference times the reference algorithm on the
+host cores instead (the CPU oracle, since Funicular.jl is Julia and Julia is
+not available here), on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cholqr2! GB/s & % roofline, tensor vs FP64 form at ||QᴴQ-I||<=1e-12"
+UNIT = "GB/s"
+N_DEFAULT, K_DEFAULT, W_PANEL = 10_000_000, 64, 16
+CPU_SAMPLE_ROWS = 1 << 21
+
+# DRAM bytes per row each kernel moved in its committed ncu capture (N = 5e5,
+# k = 64, profiles/*_N5e5_k64_ncu.md), scaled here to the bench's N.
+NCU_BYTES_PER_ROW = {"gram_partial+reduce": (512.0192e6 + 3.794e6) / 5e5,
+                     "trsm_rows": (519.448e6 + 454.977e6) / 5e5}
+NCU_CAPTURE_K = 64
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--N", type=int, default=N_DEFAULT)
+    p.add_argument("--k", type=int, default=K_DEFAULT)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--skip-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def alg_bytes(N, k):
+    return 96 * N * k  # 2 passes x (Gram read + TRSM read + TRSM write) x 16 B
+
+
+def alg_flops(N, k):
+    return 16 * N * k * k  # 2 passes x (Hermitian Gram 4Nk^2 + TRSM 4Nk^2)
+
+
+def workload_config(N, k, extra=None):
+    cfg = {
+        "workload": f"cholqr2! device-resident, N={N}, k={k}, panel width {W_PANEL}, ComplexF64, "
+                    "Y = U diag(logspace(0,-6,k)) V^H (seeded U Gaussian orthonormalized, V Haar)",
+        "N": N, "k": k, "panel_width": W_PANEL, "form": "fp64",
+        "l2": "inputs larger than L2 (10.24 GB vs 126 MB), no flush",
+        "parallelism": "replicas (one matrix per GPU)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference algorithm restated by the oracle, on host cores.
+
+def cpu_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads", 0) for i in threadpool_info() if i.get("internal_api") in ("openblas", "mkl", "blis")]
+        if n:
+            return max(n)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def cpu_cholqr2_rate(Y0: np.ndarray, steps: int, warmup: int):
+    """Times the oracle's cholqr2! (the reference's row-block order, BLAS and
+    LAPACK on every host core) on Y0; returns (GB/s, seconds per step)."""
+    from oracle import panel_oracle as oracle
+    N, k = Y0.shape
+    Y = Y0.copy(order="F")
+    for _ in range(warmup):
+        oracle.cholqr2(Y, W_PANEL)
+    times = []
+    for _ in range(steps):
+        np.copyto(Y, Y0)
+        t0 = time.perf_counter()
+        oracle.cholqr2(Y, W_PANEL)
+        times.append(time.perf_counter() - t0)
+    sec = statistics.mean(times)
+    return alg_bytes(N, k) / sec / 1e9, sec
+
+
+def synthetic_host_sample(rows, k, seed=0xDEADBEEF):
+    """The workload's matrix family on the host, for the CPU-side sample."""
+    rng = np.random.default_rng(seed)
+    G = (rng.standard_normal((rows, k)) + 1j * rng.standard_normal((rows, k))) / np.sqrt(2)
+    U, _ = np.linalg.qr(G)
+    V = haar_unitary(k, seed + 1)
+    s = 10.0 ** np.linspace(0, -6, k)
+    return np.asfortranarray((U * s) @ V.conj().T)
+
+
+def haar_unitary(k, seed):
+    rng = np.random.default_rng(seed)
+    Z = (rng.standard_normal((k, k)) + 1j * rng.standard_normal((k, k))) / np.sqrt(2)
+    Q, R = np.linalg.qr(Z)
+    d = np.diag(R)
+    return Q * (d / np.abs(d))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    k = args.k
+    rows = min(args.N, CPU_SAMPLE_ROWS)
+    Y0 = synthetic_host_sample(rows, k)
+    steps = max(1, args.steps)
+    gbs, sec = cpu_cholqr2_rate(Y0, steps=steps, warmup=max(0, min(args.warmup, 1)))
+    cores = cpu_threads()
+    sample = f"{rows} of the {args.N} rows (k={k}), {steps} timed steps of {sec:.3f} s"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.N, k, {"cpu_sample_rows": rows}),
+        "cpu_baseline": {"value": gbs, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": gbs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "Funicular.jl is Julia, which is not installed; this is the CPU oracle's restatement of its "
+                "CPU backend path (row-block order, zgemm/ztrsm/zpotrf from OpenBLAS/LAPACK).",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU side.
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device_index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._handle = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._handle, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # reported, not fatal
+            self._nvml = None
+            self.error = str(e)
+
+    def _run(self):
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._handle, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._handle)
+                for bit, name in self.REASONS.items():
+                    if mask & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self._nvml is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measure_fp64_peak(torch, device):
+    """cuBLAS ZGEMM (complex FP64, the arithmetic of this path) through torch,
+    best of a few 4096^3 products: the FP64 roofline denominator."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device=device)
+    b = torch.randn(n, n, dtype=torch.complex128, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 8 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def wrap(fb, tensor, rows, cols):
+    """A column-major DeviceMatrix over a (cols, rows) row-major torch tensor."""
+    import numpy as _np
+    return fb.DeviceMatrix(tensor.data_ptr(), (rows, cols), rows, _np.dtype(_np.complex128), tensor)
+
+
+def build_workload(fb, backend, torch, device, N, k, seed):
+    """Y = U diag(s) V^H on the device. U: a seeded complex Gaussian made
+    orthonormal by the backend's own cholqr2!; V: seeded Haar unitary."""
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    Ut = torch.randn((k, N), dtype=torch.complex128, device=device, generator=gen)
+    U = wrap(fb, Ut, N, k)
+    Rtmp = backend.alloc_device(np.complex128, (k, k))
+    fb.kernels.cholqr2_resident(backend, U, Rtmp)
+    V = haar_unitary(k, seed + 1)
+    s = 10.0 ** np.linspace(0, -6, k)
+    C = backend.todevice(np.asfortranarray(s[:, None] * V.conj().T))
+    Yt = torch.empty((k, N), dtype=torch.complex128, device=device)
+    Y = wrap(fb, Yt, N, k)
+    fb.kernels.rightmul_gemm(backend, Y, U, C)
+    backend.sync_all()
+    del U, Ut
+    return Yt
+
+
+def accuracy(fb, backend, torch, Yt0, Qt, R, N, k):
+    """||Q^H Q - I||_F (with the backend's Gram) and ||Y - Q R||_F / ||Y||_F."""
+    Q = wrap(fb, Qt, N, k)
+    G = backend.alloc_device(np.complex128, (k, k))
+    fb.kernels.gram_accumulate(backend, G, Q, Q, 1.0, 0.0)
+    orth = float(np.linalg.norm(G.to_host() - np.eye(k)))
+    QRt = torch.empty_like(Qt)
+    fb.kernels.rightmul_gemm(backend, wrap(fb, QRt, N, k), Q, R)
+    backend.sync_all()
+    QRt.sub_(Yt0)
+    recon = float(torch.linalg.vector_norm(QRt).item() / torch.linalg.vector_norm(Yt0).item())
+    del QRt
+    return orth, recon
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import __graft_entry__
+    fb = __graft_entry__.load()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    N, k = args.N, args.k
+    backend = fb.B200Backend(local)
+    fp64_peak = measure_fp64_peak(torch, device)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    hbm_source = "MEASURED_PEAKS.json" if os.path.exists(peaks_path) else "fallback"
+
+    Yt0 = build_workload(fb, backend, torch, device, N, k, seed=0xDEADBEEF + rank)
+    Yt = Yt0.clone()
+    Y = wrap(fb, Yt, N, k)
+    R = backend.alloc_device(np.complex128, (k, k))
+
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+
+    # One checked run on the true Y: accuracy and the number of passes.
+    checked = {}
+    backend.submit(queue, lambda: checked.update(r=fb.kernels.cholqr2_resident(backend, Y, R)))
+    passes, _ = checked["r"]
+    orth, recon = accuracy(fb, backend, torch, Yt0, Yt, R, N, k)
+
+    def step():
+        backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, R, wait=False))
+
+    for _ in range(args.warmup):
+        step()
+    backend.sync_queue(queue)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    launches0 = fb._lib.kernel_launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    launches = fb._lib.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms_total / args.steps
+    value = world * alg_bytes(N, k) * args.steps / (ms_total * 1e-3) / 1e9
+
+    # Per-kernel durations, same shapes as inside the step, same queue.
+    def time_kernel(fn, reps):
+        fn()
+        backend.sync_queue(queue)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    G = backend.alloc_device(np.complex128, (k, k))
+    reps = max(3, min(args.steps, 20))
+    gram_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.gram_accumulate(backend, G, Y, Y, 1.0, 0.0)), reps)
+    Rid = backend.todevice(np.asfortranarray(np.eye(k, dtype=np.complex128)))
+    trsm_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.rdiv_upper(backend, Y, Rid)), reps)
+    kernel_flops = 4 * N * k * k  # each of them, algorithmic
+    kernels = {
+        "gram_partial+reduce": {"ms": gram_ms, "tflops": kernel_flops / (gram_ms * 1e-3) / 1e12,
+                                "gbs": 16 * N * k / (gram_ms * 1e-3) / 1e9},
+        "trsm_rows": {"ms": trsm_ms, "tflops": kernel_flops / (trsm_ms * 1e-3) / 1e12,
+                      "gbs": 32 * N * k / (trsm_ms * 1e-3) / 1e9},
+    }
+    dominant = "trsm_rows" if trsm_ms >= gram_ms else "gram_partial+reduce"
+    dk = kernels[dominant]
+    traffic = NCU_BYTES_PER_ROW[dominant] * N if k == NCU_CAPTURE_K else None
+    roofline = {
+        "bound": "fp64", "achieved": dk["tflops"], "peak": fp64_peak, "unit": "TFLOP/s",
+        "frac": dk["tflops"] / fp64_peak, "traffic": traffic, "kernel": dominant,
+        "traffic_source": "ncu dram bytes of the N=5e5 capture in profiles/, scaled by N/5e5",
+        "peak_source": "cuBLAS ZGEMM 4096^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
+        "per_launch": f"4 N k^2 = {kernel_flops:.3e} flops per launch",
+    }
+    step_flops_bound = alg_flops(N, k) / (fp64_peak * 1e12) * 1e3
+    step_bytes_bound = alg_bytes(N, k) / (hbm_peak * 1e9) * 1e3
+    step_roofline = {
+        "ms_fp64_bound": step_flops_bound, "ms_hbm_bound": step_bytes_bound,
+        "ms_roofline": max(step_flops_bound, step_bytes_bound), "ms_measured": ms_step,
+        "frac": max(step_flops_bound, step_bytes_bound) / ms_step,
+        "achieved_tflops": alg_flops(N, k) / (ms_step * 1e-3) / 1e12,
+        "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_source, "fp64_peak_tflops": fp64_peak,
+    }
+
+    # End to end through host buffers: per step, Y goes up from page-locked
+    # host memory, cholqr2! runs, and Q and R come back down.
+    e2e = None
+    if args.e2e_steps > 0:
+        nbytes = N * k * 16
+        slab_in = backend.alloc_host_slab(nbytes)
+        slab_out = backend.alloc_host_slab(nbytes)
+        Yh = slab_in.matrix(np.complex128, (N, k))
+        Qh = slab_out.matrix(np.complex128, (N, k))
+        Rh = np.empty((k, k), dtype=np.complex128, order="F")
+        backend.d2h(Yh, wrap(fb, Yt0, N, k))
+
+        def e2e_step():
+            backend.h2d(Y, Yh, queue=queue)
+            backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, R, wait=False))
+            backend.d2h(Qh, Y, queue=queue)
+            backend.d2h(Rh, R, queue=queue)
+
+        e2e_step()
+        backend.sync_queue(queue)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        b.record(stream)
+        b.synchronize()
+        wall = time.perf_counter() - t0
+        ms_e2e = max_over_ranks(a.elapsed_time(b)) / args.e2e_steps
+        e2e = {"value": world * alg_bytes(N, k) / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + k * k * 16,
+               "ms_per_step": ms_e2e, "steps": args.e2e_steps, "wall_s": wall,
+               "path": "h2d! of Y from page-locked host memory, device cholqr2!, d2h! of Q and R"}
+        del slab_in, slab_out, Yh, Qh
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        rows = min(N, CPU_SAMPLE_ROWS)
+        sample = np.asfortranarray(wrap(fb, Yt0, N, k).view(slice(0, rows)).to_host())
+        gbs, sec = cpu_cholqr2_rate(sample, steps=2, warmup=0)
+        cpu = {"value": gbs, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+               "sample": f"first {rows} rows of the workload (k={k}), 2 timed steps of {sec:.3f} s each"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(N, k),
+        "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
+        "accuracy": {"orthogonality_fro": orth, "reconstruction_rel": recon, "passes": passes,
+                     "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
+        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

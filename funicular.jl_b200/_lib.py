@@ -73,6 +73,7 @@ _pvp = ctypes.POINTER(ctypes.c_void_p)
 SIGNATURES = {
     "fb_abi_version": [],
     "fb_last_error": [],
+    "fb_kernel_launches": [],
     "fb_device_count": [_pint],
     "fb_set_device": [_int],
     "fb_alloc_device": [_pvp, _sz],
@@ -102,7 +103,8 @@ SIGNATURES = {
     "fb_zcholqr2": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zcholqr2_query": [_vp, _pint, _pint, _pdbl],
 }
-_RESTYPES = {"fb_last_error": ctypes.c_char_p, "fb_abi_version": ctypes.c_int}
+_RESTYPES = {"fb_last_error": ctypes.c_char_p, "fb_abi_version": ctypes.c_int,
+             "fb_kernel_launches": ctypes.c_uint64}
 
 _lock = threading.Lock()
 _lib = None
@@ -143,6 +145,11 @@ def check(status: int, what: str = "") -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(load(), name)(*args), name)
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched in this process."""
+    return int(load().fb_kernel_launches())
 
 
 def device_count() -> int:

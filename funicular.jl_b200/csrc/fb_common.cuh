@@ -16,6 +16,8 @@ namespace fb {
 void set_error(int status, const char* fmt, ...);
 int cuda_status(cudaError_t err, const char* what);
 int sm_count();
+// Every kernel launch of this library goes through FB_LAUNCHED, which counts it.
+void count_launch();
 
 #define FB_TRY(expr)                       \
     do {                                   \
@@ -34,7 +36,11 @@ int sm_count();
 // Checks the launch that was just issued. Only the launch configuration is
 // checked here: errors raised while the kernel runs surface at the next
 // synchronizing call on the queue.
-#define FB_LAUNCHED(what) FB_CUDA(cudaGetLastError(), what)
+#define FB_LAUNCHED(what)                  \
+    do {                                   \
+        ::fb::count_launch();              \
+        FB_CUDA(cudaGetLastError(), what); \
+    } while (0)
 
 inline cudaStream_t stream_of(fb_queue_t q) { return reinterpret_cast<cudaStream_t>(q); }
 

@@ -3,6 +3,7 @@
 // as the reference's CUDA extension implements it
 // (ext/FunicularCUDAExt.jl:29-182), without any per-array stream bookkeeping:
 // ordering between queues is the caller's events alone.
+#include <atomic>
 #include <cstdarg>
 #include <mutex>
 #include <vector>
@@ -12,6 +13,9 @@
 namespace fb {
 
 static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(int status, const char* fmt, ...) {
     char buf[1024];
@@ -52,6 +56,8 @@ extern "C" {
 int fb_abi_version(void) { return FB_ABI_VERSION; }
 
 const char* fb_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t fb_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int fb_device_count(int* count) {
     if (!count) { set_error(FB_EINVAL, "fb_device_count: count is NULL"); return FB_EINVAL; }

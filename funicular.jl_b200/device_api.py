@@ -93,7 +93,8 @@ class DeviceMatrix:
             raise ArgumentError("a device view takes unit-stride ranges of rows and columns")
         r1, c1 = max(r1, r0), max(c1, c0)
         ptr = self.ptr + (r0 + c0 * self.ld) * self.itemsize
-        return DeviceMatrix(ptr, (r1 - r0, c1 - c0), self.ld, self.dtype, self.owner or self)
+        return DeviceMatrix(ptr, (r1 - r0, c1 - c0), self.ld, self.dtype,
+                            self.owner if self.owner is not None else self)
 
     def __getitem__(self, key):
         rows, cols = key

@@ -57,6 +57,8 @@ typedef void* fb_event_t;
 int fb_abi_version(void);
 /* The message of the last failing call on this host thread ("" if none). */
 const char* fb_last_error(void);
+/* Kernels this library has launched in this process, all devices together. */
+uint64_t fb_kernel_launches(void);
 /* Number of visible CUDA devices (0 on a machine without a GPU). */
 int fb_device_count(int* count);
 int fb_set_device(int device);

@@ -86,11 +86,16 @@ def choose_panel_width(N, k, itemsize, device_budget, nbuffers=2, extra_buffers=
 def gram_accumulate(C, A, B, alpha, beta):
     """gram_accumulate! (src/kernels.jl:22-55): C <- alpha A^H B + beta C, a
     zero beta overwriting C (NaN-safe)."""
+    if A.shape[0] == 0:
+        C[...] = 0 if beta == 0 else beta * C
+        return C
+    if np.iscomplexobj(A) and A.dtype == np.complex128:
+        # mul!(C, A', B, alpha, beta) reaches zgemm('C', 'N', ...)
+        out = blas.zgemm(alpha, A, B, beta=beta, c=None if beta == 0 else np.asfortranarray(C), trans_a=2)
+        C[...] = out
+        return C
     prod = A.conj().T @ B
-    if beta == 0:
-        C[...] = alpha * prod
-    else:
-        C[...] = alpha * prod + beta * C
+    C[...] = alpha * prod if beta == 0 else alpha * prod + beta * C
     return C
 
 
@@ -100,7 +105,10 @@ def rdiv_upper(Y, R):
     if Y.size == 0:
         return Y
     trsm = blas.ztrsm if np.iscomplexobj(Y) else blas.dtrsm
-    Y[...] = trsm(1.0, np.asfortranarray(R), np.asfortranarray(Y), side=1, lower=0, trans_a=0, diag=0)
+    if Y.flags.f_contiguous and Y.dtype == R.dtype:
+        trsm(1.0, np.asfortranarray(R), Y, side=1, lower=0, trans_a=0, diag=0, overwrite_b=1)
+    else:
+        Y[...] = trsm(1.0, np.asfortranarray(R), np.asfortranarray(Y), side=1, lower=0, trans_a=0, diag=0)
     return Y
 
 
@@ -112,17 +120,35 @@ def rightmul_gemm(dst, A, C):
 
 # ---- panel BLAS: src/panelblas.jl --------------------------------------------
 
+def _staging(h, cols, dtype):
+    """A sweep's staging buffer (src/executor.jl:177-182): one row block,
+    column major, as the CPU backend's "device" array."""
+    return np.empty((h, cols), dtype=dtype, order="F")
+
+
 def gram(X, Y=None, w=None):
     """gram(X[, Y]) (src/panelblas.jl:33-53): C = X^H Y accumulated one row
-    block at a time, the first block overwriting (carry, :59)."""
+    block at a time, the first block overwriting (carry, :59). Each block is
+    first copied into a staging buffer, as materialize_rows! does
+    (src/panels.jl:437-445)."""
     N, k = X.shape
     w = k if w is None else w
     same = Y is None or Y is X
     Y = X if Y is None else Y
     C = np.empty((k, Y.shape[1]), dtype=X.dtype)
-    for step, (r0, r1) in enumerate(row_blocks(N, k, w)):
-        Xb = X[r0:r1]
-        Yb = Xb if same else Y[r0:r1]
+    blocks = row_blocks(N, k, w)
+    h = blocks[0][1] - blocks[0][0]
+    xs = _staging(h, k, X.dtype)
+    ys = xs if same else _staging(h, Y.shape[1], Y.dtype)
+    for step, (r0, r1) in enumerate(blocks):
+        n = r1 - r0
+        Xb = xs if n == h else xs[:n]
+        np.copyto(Xb, X[r0:r1])
+        if same:
+            Yb = Xb
+        else:
+            Yb = ys if n == h else ys[:n]
+            np.copyto(Yb, Y[r0:r1])
         gram_accumulate(C, Xb, Yb, 1.0, 0.0 if step == 0 else 1.0)
     return C
 
@@ -149,8 +175,15 @@ def rdiv_rows(Y, R, w=None):
     time."""
     N, k = Y.shape
     w = k if w is None else w
-    for r0, r1 in row_blocks(N, k, w):
-        rdiv_upper(Y[r0:r1], R)
+    blocks = row_blocks(N, k, w)
+    h = blocks[0][1] - blocks[0][0]
+    ys = _staging(h, k, Y.dtype)
+    for r0, r1 in blocks:
+        n = r1 - r0
+        Yb = ys if n == h else ys[:n]
+        np.copyto(Yb, Y[r0:r1])
+        rdiv_upper(Yb, R)
+        np.copyto(Y[r0:r1], Yb)
     return Y
 
 

@@ -22,6 +22,9 @@
 // with the columns permuted, column 4*m + c stored at c*nm + m, so that the
 // threads of a warp, which read four columns 4*m..4*m+3 for different m,
 // touch consecutive 16-byte words and never share a bank.
+#include <mutex>
+#include <vector>
+
 #include "fb_common.cuh"
 
 namespace fb {
@@ -369,6 +372,33 @@ size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian) {
     return gram_workspace_bytes(gram_shape(rows, kA, kB, hermitian ? 1 : 0));
 }
 
+// Scratch for fb_zgram_static, the entry point for callers that cannot
+// allocate device memory. It is an ordinary global of this module, so every
+// GPU that loads the library holds these bytes until the process exits. The
+// partial tiles it holds are written by each call before that call reads
+// them, so nothing in it has to start at zero.
+constexpr size_t GRAM_STATIC_SCRATCH_BYTES = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_gram_static_scratch[GRAM_STATIC_SCRATCH_BYTES];
+
+// The device address of g_gram_static_scratch on the current device. Host
+// code sees the symbol's name only as a host-side stand-in, so the address is
+// asked of the runtime once per device (with that device current) and cached.
+static int gram_static_scratch(void** out) {
+    static std::mutex mu;
+    static std::vector<void*> addresses;
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)addresses.size() <= dev) addresses.resize(dev + 1, nullptr);
+    if (addresses[dev] == nullptr) {
+        void* p = nullptr;
+        FB_CUDA(cudaGetSymbolAddress(&p, g_gram_static_scratch), "cudaGetSymbolAddress(g_gram_static_scratch)");
+        addresses[dev] = p;
+    }
+    *out = addresses[dev];
+    return FB_OK;
+}
+
 }  // namespace fb
 
 using namespace fb;
@@ -407,6 +437,41 @@ int fb_zgram(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda, const fb_z1
     return gram_enqueue(reinterpret_cast<z64*>(C), ldc, reinterpret_cast<const z64*>(A), lda,
                         reinterpret_cast<const z64*>(B), ldb, rows, kA, kB, a, b, hermitian,
                         workspace, workspace_bytes, stream_of(queue), nullptr, GATE_ALWAYS);
+}
+
+int fb_zgram_static(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda, const fb_z128* B, int64_t ldb,
+                    int64_t rows, int kA, int kB, fb_z128 alpha, fb_z128 beta, fb_queue_t queue) {
+    if (rows < 0 || kA < 0 || kB < 0) {
+        set_error(FB_EDIM, "cannot accumulate a product with negative sizes (rows=%lld, kA=%d, kB=%d)",
+                  (long long)rows, kA, kB);
+        return FB_EDIM;
+    }
+    if (kA == 0 || kB == 0) return FB_OK;
+    if (!C || (rows > 0 && (!A || !B))) { set_error(FB_EINVAL, "fb_zgram_static: NULL matrix"); return FB_EINVAL; }
+    if (ldc < kA || (rows > 0 && (lda < rows || ldb < rows))) {
+        set_error(FB_EDIM, "fb_zgram_static: a leading dimension is smaller than the column it holds (ldc=%lld for %d rows, lda=%lld, ldb=%lld for %lld rows)",
+                  (long long)ldc, kA, (long long)lda, (long long)ldb, (long long)rows);
+        return FB_EDIM;
+    }
+    if (((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15) {
+        set_error(FB_EINVAL, "fb_zgram_static: device pointers must be 16-byte aligned");
+        return FB_EINVAL;
+    }
+    const bool hermitian = (A == B) && (lda == ldb) && (kA == kB);
+    const size_t need = gram_workspace_size(rows, kA, kB, hermitian);
+    if (need > GRAM_STATIC_SCRATCH_BYTES) {
+        set_error(FB_ENOMEM,
+                  "fb_zgram_static: a %d x %d Gram over %lld rows needs %zu bytes of scratch, more than the %zu bytes "
+                  "this entry point holds; use fb_zgram with a workspace of fb_zgram_workspace_size bytes",
+                  kA, kB, (long long)rows, need, GRAM_STATIC_SCRATCH_BYTES);
+        return FB_ENOMEM;
+    }
+    void* scratch = nullptr;
+    FB_TRY(gram_static_scratch(&scratch));
+    z64 a = zmake(alpha.re, alpha.im), b = zmake(beta.re, beta.im);
+    return gram_enqueue(reinterpret_cast<z64*>(C), ldc, reinterpret_cast<const z64*>(A), lda,
+                        reinterpret_cast<const z64*>(B), ldb, rows, kA, kB, a, b, hermitian,
+                        scratch, GRAM_STATIC_SCRATCH_BYTES, stream_of(queue), nullptr, GATE_ALWAYS);
 }
 
 }  // extern "C"

@@ -133,6 +133,28 @@ int fb_zgram(fb_z128* C, int64_t ldc,
              int64_t rows, int kA, int kB, fb_z128 alpha, fb_z128 beta,
              void* workspace, size_t workspace_bytes, fb_queue_t queue);
 
+/* gram_accumulate! for callers that cannot allocate device memory. No
+ * counterpart in the reference. fb_zgram needs a workspace from its caller;
+ * some callers have none to give: a host whose allocator has promised every
+ * device byte to a budgeted pool (a Funicular plan checks each buffer against
+ * device_budget, and its sweep loop must not allocate at all), or a host that
+ * cannot afford cudaMalloc's implicit device synchronization in the middle of
+ * a pipelined sweep. This entry point computes the same thing as fb_zgram,
+ * with the same bits, but keeps its partial tiles in a scratch array built
+ * into the library: 16 MiB, held on every GPU that loads the library until
+ * the process exits. Shapes whose scratch would not fit in it
+ * (fb_zgram_workspace_size above 16 MiB, which takes many 64 x 64 output
+ * tiles: every Gram of at most 128 columns fits) are refused with FB_ENOMEM
+ * before anything is enqueued. The first call on each device looks up the array's device
+ * address; make it before any stream capture begins. All calls share the one
+ * array: two calls whose work can overlap on the GPU (different queues with no
+ * event ordering them) race on it, while calls on one queue are safe. Each
+ * call writes every part of the array it reads, so nothing has to be cleared
+ * between calls. The call allocates nothing. */
+int fb_zgram_static(fb_z128* C, int64_t ldc,
+                    const fb_z128* A, int64_t lda, const fb_z128* B, int64_t ldb,
+                    int64_t rows, int kA, int kB, fb_z128 alpha, fb_z128 beta, fb_queue_t queue);
+
 /* rdiv_upper!(backend, Y, R) (src/kernels.jl:108): Y <- Y R^-1 in place for
  * an upper triangular, non-unit k x k R; Y is rows x k with leading
  * dimension ldy (a row block view of a staging buffer is fine). */

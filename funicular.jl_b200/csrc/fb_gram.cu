@@ -2,54 +2,65 @@
 // skinny A (rows x kA) and B (rows x kB), ComplexF64, FP64 throughout.
 //
 // Layout of the work. C is cut into tiles of at most 64 x 64 columns. A CTA
-// owns one tile and one chunk of rows. It streams its rows through shared
-// memory in stages of 32 rows (cp.async, zero-filled past the last row and
-// the last column, so ragged views need no special case), and every thread
-// accumulates a 4 x 4 block of the tile in registers over the whole chunk.
-// The threads of a CTA form several row groups that cover the tile each, so
-// the thread count is a whole number of warps for every tile shape. At the
-// end the row groups are summed in a fixed order and the CTA's partial tile
-// goes to the workspace; a second kernel adds the chunks, again in a fixed
-// order, and applies alpha and beta. Nothing depends on timing, so the bits
-// of the result depend only on (rows, kA, kB) and the device's SM count.
+// owns one tile and one chunk of rows, which it streams through shared memory
+// in stages of 32 rows: one producer warp issues TMA loads (boxes of 8 rows x
+// the tile's columns, 128-byte swizzled, zero-filled past the last row and
+// column, so ragged views need no special code) into a ring of stages guarded
+// by mbarriers, and the consumer warps multiply. The products run on the FP64
+// tensor cores (mma m8n8k4): with W the real matrix whose rows are the real
+// and imaginary parts of Y's rows, Re(A^H B) = W_A^T W_B and
+// Im(A^H B) = (J W_A)^T W_B, J taking each (re, im) pair to (-im, re). So
+// an 8 x 8 block of C costs two MMAs per two complex rows, and the J costs
+// only a register select: the A fragment's 16-byte load holds both parts, and
+// a warp loads it once for all its blocks in the same block row.
+// Every consumer warp owns whole 8 x 8 blocks of the tile for the whole
+// chunk, so nothing is reduced across warps. A warp's blocks accumulate in
+// registers; at the end the CTA's partial tile goes to the workspace, and a
+// second kernel adds the chunks in a fixed order and applies alpha and beta.
+// Nothing depends on timing, so the bits of the result depend only on
+// (rows, kA, kB) and the device.
 //
 // When A and B are the same view the tile grid is folded: only tiles on or
-// above the diagonal run, and inside a diagonal tile only the 4 x 4 blocks on
-// or above the diagonal. The lower triangle is written as the conjugate of the
-// upper one and the diagonal is made real.
+// above the diagonal run and, inside a diagonal tile, only 8 x 8 blocks on or
+// above the diagonal (36 of 64 at k = 64). The lower triangle is written as
+// the conjugate of the upper one and the diagonal is made real.
 //
-// Shared memory holds each stage row-major (one row of the tile contiguous)
-// with the columns permuted, column 4*m + c stored at c*nm + m, so that the
-// threads of a warp, which read four columns 4*m..4*m+3 for different m,
-// touch consecutive 16-byte words and never share a bank.
+// Swizzle: a TMA box is 8 rows (128 bytes per column) by the tile's columns,
+// and 128-byte swizzling stores the 16-byte element of row r in column c at
+// chunk r ^ (c % 8) of that column's 128-byte line. The eight lanes that read
+// eight consecutive columns of one row therefore hit eight different banks.
 #include <mutex>
 #include <vector>
 
 #include "fb_common.cuh"
+#include "fb_tma.cuh"
 
 namespace fb {
 
-constexpr int GS_ROWS = 32;
-constexpr int GS_STAGES = 3;
-constexpr int G_TILE = 64;
-constexpr int G_MAX_THREADS = 576;
+constexpr int GS_ROWS = 32;             // complex rows per stage
+constexpr int GS_BOX_ROWS = 8;          // complex rows per TMA box (128 bytes)
+constexpr int GS_BOXES = GS_ROWS / GS_BOX_ROWS;
+constexpr int G_TILE = 64;              // columns per output tile side, at most
+constexpr int G_MAX_WARPS = 17;         // 16 consumers + the producer
 
 struct GramShape {
-    int tw_a, tw_b;      // tile widths in columns (multiples of 4, at most 64)
+    int tw_a, tw_b;      // tile widths in columns (multiples of 8, at most 64)
     int nt_a, nt_b;      // tiles along the columns of A and of B
     int hermitian;
     int ntiles;          // tiles in the partial buffer
-    int64_t chunk_rows;
+    int64_t chunk_rows;  // a multiple of GS_ROWS
     int nchunks;
 };
 
 struct GramLaunch {
     int diag;            // folded diagonal tiles (hermitian mode)
     int ntiles;          // CTAs along x
-    int nm_a, nm_b;      // 4-column micro blocks per tile side
-    int micro;           // micro blocks a row group covers
-    int groups;          // row groups
-    int threads;
+    int nb_a, nb_b;      // 8-column blocks per tile side
+    int npairs;          // 8 x 8 blocks of the tile that are computed
+    int ppw;             // blocks per consumer warp
+    int consumers;       // consumer warps
+    int stages;
+    int stage_bytes;
     size_t smem;
 };
 
@@ -59,22 +70,16 @@ __host__ __device__ inline int off_tile_index(int nt, int ti, int tj) {
     return nt + ti * (2 * nt - ti - 1) / 2 + (tj - ti - 1);
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
-    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    int src_size = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_size));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
-__global__ void __launch_bounds__(G_MAX_THREADS, 1)
-gram_partial_kernel(const z64* __restrict__ A, int64_t lda, const z64* __restrict__ B, int64_t ldb,
-                    int64_t rows, int kA, int kB, GramShape sh, GramLaunch ln,
-                    z64* __restrict__ partial, const ChainStatus* st, int gate) {
+// Consumer warps per block count: at most 16 with two blocks a warp, 12 with
+// three, 8 with eight. Fewer warps leave each more registers.
+template <int PPW>
+__global__ void __launch_bounds__(PPW >= 8 ? 9 * 32 : PPW == 3 ? 13 * 32 : G_MAX_WARPS * 32, 1)
+gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 int64_t rows, GramShape sh, GramLaunch ln, z64* __restrict__ partial,
+                 const ChainStatus* st, int gate) {
     if (gated_off(st, gate)) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    z64* smem = reinterpret_cast<z64*>(smem_raw);
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 
     // Which tile this CTA owns.
     int ti, tj, tile_index;
@@ -95,136 +100,164 @@ gram_partial_kernel(const z64* __restrict__ A, int64_t lda, const z64* __restric
     const int chunk = blockIdx.y;
     const int64_t row0 = (int64_t)chunk * sh.chunk_rows;
     const int64_t row_end = min(rows, row0 + sh.chunk_rows);
-    const int col_a0 = ti * sh.tw_a, col_b0 = tj * sh.tw_b;
-    const bool same = ln.diag != 0;  // B tile is the A tile
-    const int tw_a = sh.tw_a, tw_b = sh.tw_b;
-    const int stride_a = tw_a + 1, stride_b = tw_b + 1;
-    const int stage_a = GS_ROWS * stride_a, stage_b = same ? 0 : GS_ROWS * stride_b;
-    const int stage_elems = stage_a + stage_b;
+    const int64_t nstages = (row_end - row0 + GS_ROWS - 1) / GS_ROWS;
+    const int box_a = sh.tw_a * 128, box_b = ln.diag ? box_a : sh.tw_b * 128;
+    const int stages = ln.stages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)stages * ln.stage_bytes);
+    uint64_t* empty = full + stages;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    // This thread's 4 x 4 block and row group.
-    const int tid = threadIdx.x;
-    const int g = tid / ln.micro;
-    const int m = tid - g * ln.micro;
-    const bool computes = g < ln.groups;
-    int mi = 0, mj = 0;
-    if (computes) {
-        if (ln.diag) {
-            int r = m;
-            while (r >= ln.nm_a - mi) { r -= ln.nm_a - mi; ++mi; }
-            mj = mi + r;
-        } else {
-            mi = m / ln.nm_b;
-            mj = m - mi * ln.nm_b;
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < stages; ++b) {
+            mbar_init(&full[b], 1);
+            mbar_init(&empty[b], ln.consumers);
         }
+        mbar_fence_init();
     }
-    const int rows_per_group = GS_ROWS / ln.groups;
-
-    z64 acc[4][4];
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) acc[x][y] = zmake(0.0, 0.0);
-
-    const int64_t nstages = (row_end > row0) ? (row_end - row0 + GS_ROWS - 1) / GS_ROWS : 0;
-
-    auto load_stage = [&](int64_t s, int buf) {
-        z64* sa = smem + buf * stage_elems;
-        z64* sb = same ? sa : sa + stage_a;
-        const int64_t r0 = row0 + s * GS_ROWS;
-        const int total_a = GS_ROWS * tw_a;
-        for (int e = tid; e < total_a; e += blockDim.x) {
-            int l = e & (GS_ROWS - 1), c = e >> 5;
-            int64_t r = r0 + l;
-            int col = col_a0 + c;
-            bool valid = (r < row_end) && (col < kA);
-            const z64* src = valid ? (A + r + (int64_t)col * lda) : A;
-            int phys = (c & 3) * ln.nm_a + (c >> 2);
-            cp_async16(sa + l * stride_a + phys, src, valid);
-        }
-        if (!same) {
-            const int total_b = GS_ROWS * tw_b;
-            for (int e = tid; e < total_b; e += blockDim.x) {
-                int l = e & (GS_ROWS - 1), c = e >> 5;
-                int64_t r = r0 + l;
-                int col = col_b0 + c;
-                bool valid = (r < row_end) && (col < kB);
-                const z64* src = valid ? (B + r + (int64_t)col * ldb) : B;
-                int phys = (c & 3) * ln.nm_b + (c >> 2);
-                cp_async16(sb + l * stride_b + phys, src, valid);
-            }
-        }
-    };
-
-    // Prologue: fill GS_STAGES - 1 stages.
-#pragma unroll
-    for (int s = 0; s < GS_STAGES - 1; ++s) {
-        if (s < nstages) load_stage(s, s);
-        cp_async_commit();
-    }
-
-    for (int64_t s = 0; s < nstages; ++s) {
-        cp_async_wait<GS_STAGES - 2>();
-        __syncthreads();
-        // Refill the buffer the previous iteration finished with.
-        {
-            int64_t nxt = s + GS_STAGES - 1;
-            if (nxt < nstages) load_stage(nxt, (int)(nxt % GS_STAGES));
-            cp_async_commit();
-        }
-        if (computes) {
-            const z64* sa = smem + (int)(s % GS_STAGES) * stage_elems;
-            const z64* sb = same ? sa : sa + stage_a;
-            const int l0 = g * rows_per_group;
-#pragma unroll 1
-            for (int l = l0; l < l0 + rows_per_group; ++l) {
-                z64 a[4], b[4];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) a[c] = sa[l * stride_a + c * ln.nm_a + mi];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) b[c] = sb[l * stride_b + c * ln.nm_b + mj];
-#pragma unroll
-                for (int x = 0; x < 4; ++x)
-#pragma unroll
-                    for (int y = 0; y < 4; ++y) zmac_conj(acc[x][y], a[x], b[y]);
-            }
-        }
-    }
-    cp_async_wait<0>();
     __syncthreads();
 
-    // Sum the row groups into group 0, in group order, through shared memory.
-    z64* red = smem;
-    for (int r = 1; r < ln.groups; ++r) {
-        if (computes && g == r) {
-#pragma unroll
-            for (int x = 0; x < 4; ++x)
-#pragma unroll
-                for (int y = 0; y < 4; ++y) red[(x * 4 + y) * ln.micro + m] = acc[x][y];
-        }
-        __syncthreads();
-        if (computes && g == 0) {
-#pragma unroll
-            for (int x = 0; x < 4; ++x)
-#pragma unroll
-                for (int y = 0; y < 4; ++y) {
-                    z64 v = red[(x * 4 + y) * ln.micro + m];
-                    acc[x][y].x += v.x;
-                    acc[x][y].y += v.y;
+    if (warp == ln.consumers) {
+        // Producer: one lane keeps the ring full.
+        if (lane == 0) {
+            tma_prefetch_map(&tmA);
+            if (!ln.diag) tma_prefetch_map(&tmB);
+            // Ring slot and phase advance incrementally: a 64-bit division per
+            // stage would run on the slow XU pipe and starve the MMAs.
+            int b = 0;
+            uint32_t phase = 0;
+            for (int64_t s = 0; s < nstages; ++s) {
+                if (s >= stages && !mbar_wait(&empty[b], phase ^ 1u)) break;
+                mbar_arrive_expect_tx(&full[b], (uint32_t)ln.stage_bytes);
+                unsigned char* dst = smem + (size_t)b * ln.stage_bytes;
+                const int64_t r = row0 + s * GS_ROWS;
+                for (int g = 0; g < GS_BOXES; ++g)
+                    tma_load_2d(dst + g * box_a, &tmA, (int)(2 * (r + g * GS_BOX_ROWS)), ti * sh.tw_a, &full[b]);
+                if (!ln.diag) {
+                    unsigned char* dstb = dst + GS_BOXES * box_a;
+                    for (int g = 0; g < GS_BOXES; ++g)
+                        tma_load_2d(dstb + g * box_b, &tmB, (int)(2 * (r + g * GS_BOX_ROWS)), tj * sh.tw_b, &full[b]);
                 }
+                if (++b == stages) { b = 0; phase ^= 1u; }
+            }
         }
-        __syncthreads();
+        return;
     }
 
-    if (computes && g == 0) {
-        z64* out = partial + ((size_t)tile_index * sh.nchunks + chunk) * (G_TILE * G_TILE);
+    // Consumers: this warp's 8 x 8 blocks. A warp past the last block
+    // computes a copy of block 0 and never writes it, so the inner loop has no
+    // branch on it.
+    int bi[PPW], bj[PPW];
+    bool valid[PPW];
 #pragma unroll
-        for (int x = 0; x < 4; ++x)
+    for (int i = 0; i < PPW; ++i) {
+        int p = warp * PPW + i;
+        valid[i] = p < ln.npairs;
+        if (!valid[i]) p = 0;
+        if (ln.diag) {
+            int I = 0;
+            while (p >= ln.nb_a - I) { p -= ln.nb_a - I; ++I; }
+            bi[i] = I;
+            bj[i] = I + p;
+        } else {
+            bi[i] = p / ln.nb_b;
+            bj[i] = p - bi[i] * ln.nb_b;
+        }
+    }
+
+    // Lane roles in the m8n8k4 fragments: col8 = column within the 8-block,
+    // t = which of the k-step's two complex rows, part = re or im. A k-step
+    // takes rows q and q + 4 of a box, so the swizzled chunks of the two rows
+    // (q ^ c and (q + 4) ^ c) never share a bank within a half warp.
+    const int col8 = lane >> 2;
+    const int t = (lane >> 1) & 1;
+    const int part = lane & 1;
+    int swz[4];
 #pragma unroll
-            for (int y = 0; y < 4; ++y) {
-                int li = 4 * mi + x, lj = 4 * mj + y;
-                out[lj * G_TILE + li] = acc[x][y];
+    for (int q = 0; q < 4; ++q) swz[q] = ((q + 4 * t) ^ col8) << 4;
+    // Byte offsets within a box: the lane's own part of A and of B, and the
+    // other part of A, whose sign flip turns W_A into (J W_A) for the
+    // imaginary product (J takes (re, im) to (-im, re)).
+    int offA[PPW], offAo[PPW], offB[PPW];
+    bool newA[PPW];
+#pragma unroll
+    for (int i = 0; i < PPW; ++i) {
+        offA[i] = (bi[i] * 8 + col8) * 128 + part * 8;
+        offAo[i] = (bi[i] * 8 + col8) * 128 + (part ^ 1) * 8;
+        offB[i] = (bj[i] * 8 + col8) * 128 + part * 8;
+        newA[i] = (i == 0) || (bi[i] != bi[i > 0 ? i - 1 : 0]);
+    }
+    const unsigned long long flip = part ? 0ull : 0x8000000000000000ull;
+
+    // NACC interleaved accumulator sets (alternate k-steps) double the
+    // independent MMA chains per warp.
+    constexpr int NACC = PPW >= 8 ? 1 : 2;
+    double acc[NACC][PPW][2][2];
+#pragma unroll
+    for (int h = 0; h < NACC; ++h)
+#pragma unroll
+        for (int i = 0; i < PPW; ++i)
+            acc[h][i][0][0] = acc[h][i][0][1] = acc[h][i][1][0] = acc[h][i][1][1] = 0.0;
+
+    bool ok = true;
+    int b = 0;
+    uint32_t phase = 0;
+    for (int64_t s = 0; s < nstages; ++s) {
+        if (!mbar_wait(&full[b], phase)) { ok = false; break; }
+        const unsigned char* sa = smem + (size_t)b * ln.stage_bytes;
+        const unsigned char* sbb = ln.diag ? sa : sa + GS_BOXES * box_a;
+#pragma unroll 1
+        for (int g = 0; g < GS_BOXES; ++g) {
+            const unsigned char* ba = sa + g * box_a;
+            const unsigned char* bb = sbb + g * box_b;
+            constexpr int Q_UNROLL = PPW >= 8 ? 1 : 4;
+#pragma unroll Q_UNROLL
+            for (int q = 0; q < 4; ++q) {
+                const int h = q % NACC;
+                double are = 0.0, aim = 0.0;
+#pragma unroll
+                for (int i = 0; i < PPW; ++i) {
+                    if (newA[i]) {
+                        are = *reinterpret_cast<const double*>(ba + offA[i] + swz[q]);
+                        aim = __longlong_as_double(
+                            __double_as_longlong(*reinterpret_cast<const double*>(ba + offAo[i] + swz[q])) ^ flip);
+                    }
+                    const double bw = *reinterpret_cast<const double*>(bb + offB[i] + swz[q]);
+                    dmma_884(acc[h][i][0][0], acc[h][i][0][1], are, bw);
+                    dmma_884(acc[h][i][1][0], acc[h][i][1][1], aim, bw);
+                }
             }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[b]);
+        if (++b == stages) { b = 0; phase ^= 1u; }
+    }
+    if (!ok) {
+        // A stage never arrived: poison this CTA's share of the result so the
+        // failure reaches the caller as NaN instead of a silent wrong answer.
+#pragma unroll
+        for (int i = 0; i < PPW; ++i)
+            acc[0][i][0][0] = acc[0][i][0][1] = acc[0][i][1][0] = acc[0][i][1][1] = __longlong_as_double(0x7ff8000000000000ll);
+    }
+#pragma unroll
+    for (int h = 1; h < NACC; ++h)
+#pragma unroll
+        for (int i = 0; i < PPW; ++i)
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                acc[0][i][x][0] += acc[h][i][x][0];
+                acc[0][i][x][1] += acc[h][i][x][1];
+            }
+
+    z64* out = partial + ((size_t)tile_index * sh.nchunks + chunk) * (G_TILE * G_TILE);
+#pragma unroll
+    for (int i = 0; i < PPW; ++i) {
+        if (!valid[i]) continue;
+        const int li = bi[i] * 8 + (lane >> 2);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int lj = bj[i] * 8 + 2 * (lane & 3) + c;
+            out[lj * G_TILE + li] = zmake(acc[0][i][0][c], acc[0][i][1][c]);
+        }
     }
 }
 
@@ -267,21 +300,9 @@ __global__ void gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int kA, int
     *dst = out;
 }
 
-static int pick_groups(int micro) {
-    int best = 1;
-    for (int g = 1; g <= 32; g <<= 1) {
-        if (micro * g > G_MAX_THREADS) break;
-        best = g;
-    }
-    // Prefer a whole number of warps when a smaller group count gives one.
-    for (int g = best; g >= 1; g >>= 1)
-        if ((micro * g) % 32 == 0) return g;
-    return best;
-}
-
-static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian) {
+static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian, int ctas_per_sm) {
     GramShape sh{};
-    auto tile_width = [](int k) { int w = k < G_TILE ? k : G_TILE; return (w + 3) / 4 * 4; };
+    auto tile_width = [](int k) { int w = k < G_TILE ? k : G_TILE; return (w + 7) / 8 * 8; };
     sh.tw_a = tile_width(kA);
     sh.tw_b = tile_width(kB);
     sh.nt_a = (kA + sh.tw_a - 1) / sh.tw_a;
@@ -291,7 +312,7 @@ static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian) {
     int largest_launch = hermitian ? (sh.nt_a > 1 ? sh.nt_a * (sh.nt_a - 1) / 2 : 1) : sh.ntiles;
     if (hermitian && sh.nt_a > largest_launch) largest_launch = sh.nt_a;
     const int64_t stages = (rows + GS_ROWS - 1) / GS_ROWS;
-    int64_t target = (int64_t)sm_count() / largest_launch;
+    int64_t target = (int64_t)sm_count() * ctas_per_sm / largest_launch;
     if (target < 1) target = 1;
     if (target > stages) target = stages;
     if (target < 1) target = 1;
@@ -304,22 +325,60 @@ static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian) {
 static GramLaunch gram_launch(const GramShape& sh, bool diag) {
     GramLaunch ln{};
     ln.diag = diag;
-    ln.nm_a = sh.tw_a / 4;
-    ln.nm_b = diag ? ln.nm_a : sh.tw_b / 4;
+    ln.nb_a = sh.tw_a / 8;
+    ln.nb_b = diag ? ln.nb_a : sh.tw_b / 8;
     if (diag) {
         ln.ntiles = sh.nt_a;
-        ln.micro = ln.nm_a * (ln.nm_a + 1) / 2;
+        ln.npairs = ln.nb_a * (ln.nb_a + 1) / 2;
     } else {
         ln.ntiles = sh.hermitian ? sh.nt_a * (sh.nt_a - 1) / 2 : sh.nt_a * sh.nt_b;
-        ln.micro = ln.nm_a * ln.nm_b;
+        ln.npairs = ln.nb_a * ln.nb_b;
     }
-    ln.groups = pick_groups(ln.micro);
-    ln.threads = (ln.micro * ln.groups + 31) / 32 * 32;
-    int stage = GS_ROWS * (sh.tw_a + 1) + (diag ? 0 : GS_ROWS * (sh.tw_b + 1));
-    size_t stages_bytes = (size_t)GS_STAGES * stage * sizeof(z64);
-    size_t red_bytes = (size_t)16 * ln.micro * sizeof(z64);
-    ln.smem = stages_bytes > red_bytes ? stages_bytes : red_bytes;
+    // Blocks per warp: three (at most 12 consumer warps), two (at most 16) or
+    // eight (at most 8), whichever leaves no warp with a block to spare.
+    if (ln.npairs % 3 == 0 && ln.npairs <= 36) ln.ppw = 3;
+    else if (ln.npairs <= 32) ln.ppw = 2;
+    else ln.ppw = 8;
+    ln.consumers = (ln.npairs + ln.ppw - 1) / ln.ppw;
+    ln.stage_bytes = GS_BOXES * (sh.tw_a * 128 + (diag ? 0 : sh.tw_b * 128));
+    ln.stages = diag ? 4 : 3;
+    while (ln.stages > 2 && (size_t)ln.stages * ln.stage_bytes > 200 * 1024) --ln.stages;
+    ln.smem = (size_t)ln.stages * ln.stage_bytes + 2 * ln.stages * sizeof(uint64_t) + 1024;
     return ln;
+}
+
+template <int PPW>
+static int set_gram_attr(size_t smem) {
+    FB_CUDA(cudaFuncSetAttribute(gram_dmma_kernel<PPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "cudaFuncSetAttribute(gram_dmma_kernel)");
+    return FB_OK;
+}
+
+// CTAs of the larger launch that fit on one SM at once: the chunk count is
+// chosen from it so that one wave covers the GPU.
+static int gram_ctas_per_sm(int64_t rows, int kA, int kB, bool hermitian) {
+    GramShape sh = gram_shape(rows, kA, kB, hermitian ? 1 : 0, 1);
+    // The larger of the two launches sets the pace: the diagonal tile when
+    // there is only one, the off-diagonal tiles otherwise.
+    GramLaunch ln = gram_launch(sh, hermitian && sh.nt_a == 1);
+    int threads = (ln.consumers + 1) * 32;
+    int by_smem = (int)((227 * 1024) / (ln.smem + 1024));
+    int by_threads = 2048 / threads;
+    int by_regs = 65536 / (threads * 128);  // the consumers' register count, from ptxas
+    int n = by_smem;
+    if (by_threads < n) n = by_threads;
+    if (by_regs < n) n = by_regs;
+    return n < 1 ? 1 : n;
+}
+
+template <int PPW>
+static int launch_gram_dmma(const CUtensorMap& ma, const CUtensorMap& mb, int64_t rows, const GramShape& sh,
+                            const GramLaunch& ln, z64* partial, cudaStream_t stream, const ChainStatus* st, int gate) {
+    FB_TRY(set_gram_attr<PPW>(ln.smem));
+    dim3 grid(ln.ntiles, sh.nchunks);
+    gram_dmma_kernel<PPW><<<grid, (ln.consumers + 1) * 32, ln.smem, stream>>>(ma, mb, rows, sh, ln, partial, st, gate);
+    FB_LAUNCHED("gram_dmma_kernel");
+    return FB_OK;
 }
 
 static size_t gram_workspace_bytes(const GramShape& sh) {
@@ -331,7 +390,7 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
                  int64_t rows, int kA, int kB, z64 alpha, z64 beta, bool hermitian,
                  void* workspace, size_t workspace_bytes, cudaStream_t stream,
                  const ChainStatus* st, int gate) {
-    GramShape sh = gram_shape(rows, kA, kB, hermitian ? 1 : 0);
+    GramShape sh = gram_shape(rows, kA, kB, hermitian ? 1 : 0, gram_ctas_per_sm(rows, kA, kB, hermitian));
     size_t need = gram_workspace_bytes(sh);
     if (workspace_bytes < need || workspace == nullptr) {
         set_error(FB_ENOMEM, "gram: workspace of %zu bytes is smaller than the %zu bytes this shape needs",
@@ -340,23 +399,21 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
     }
     z64* partial = static_cast<z64*>(workspace);
     if (sh.nchunks > 0) {
+        CUtensorMap ma, mb;
+        FB_TRY(encode_panel_map(&ma, A, rows, kA, lda, sh.tw_a));
+        FB_TRY(encode_panel_map(&mb, B, rows, kB, ldb, sh.tw_b));
         const bool launches[2] = {hermitian, !hermitian || sh.nt_a > 1};
         for (int d = 0; d < 2; ++d) {
             if (!launches[d]) continue;
-            bool diag = (d == 0);
-            GramLaunch ln = gram_launch(sh, diag);
+            GramLaunch ln = gram_launch(sh, d == 0);
             if (ln.ntiles == 0) continue;
-            static bool attr_set = false;
-            if (!attr_set) {
-                FB_CUDA(cudaFuncSetAttribute(gram_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             227 * 1024),
-                        "cudaFuncSetAttribute(gram_partial_kernel)");
-                attr_set = true;
+            int status;
+            switch (ln.ppw) {
+                case 2: status = launch_gram_dmma<2>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
+                case 3: status = launch_gram_dmma<3>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
+                default: status = launch_gram_dmma<8>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
             }
-            dim3 grid(ln.ntiles, sh.nchunks);
-            gram_partial_kernel<<<grid, ln.threads, ln.smem, stream>>>(A, lda, B, ldb, rows, kA, kB, sh, ln,
-                                                                       partial, st, gate);
-            FB_LAUNCHED("gram_partial_kernel");
+            FB_TRY(status);
         }
     }
     int64_t entries = (int64_t)kA * kB;
@@ -369,7 +426,7 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
 }
 
 size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian) {
-    return gram_workspace_bytes(gram_shape(rows, kA, kB, hermitian ? 1 : 0));
+    return gram_workspace_bytes(gram_shape(rows, kA, kB, hermitian ? 1 : 0, gram_ctas_per_sm(rows, kA, kB, hermitian)));
 }
 
 // Scratch for fb_zgram_static, the entry point for callers that cannot

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "fb_common.cuh"
+#include "fb_tma.cuh"
 
 namespace fb {
 
@@ -45,6 +46,44 @@ int sm_count() {
         counts[dev] = n;
     }
     return counts[dev];
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+int encode_panel_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int64_t ld, int box_cols) {
+    auto encode = tensor_map_encoder();
+    if (!encode) {
+        set_error(FB_ECUDA, "the driver does not provide cuTensorMapEncodeTiled");
+        return FB_ECUDA;
+    }
+    if (rows < 1) rows = 1;
+    if (cols < 1) cols = 1;
+    cuuint64_t dims[2] = {(cuuint64_t)(2 * rows), (cuuint64_t)cols};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 16)};
+    cuuint32_t box[2] = {16u, (cuuint32_t)box_cols};
+    cuuint32_t elem[2] = {1u, 1u};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, elem,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error(FB_ECUDA, "cuTensorMapEncodeTiled failed (%d) for a %lld x %lld panel, ld %lld, box %d columns",
+                  (int)r, (long long)rows, (long long)cols, (long long)ld, box_cols);
+        return FB_ECUDA;
+    }
+    return FB_OK;
 }
 
 }  // namespace fb

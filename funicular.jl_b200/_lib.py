@@ -96,7 +96,8 @@ SIGNATURES = {
     "fb_zgram_workspace_size": [_i64, _int, _int, _int, _psz],
     "fb_zgram": [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, Z128, Z128, _vp, _sz, _vp],
     "fb_zgram_static": [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, Z128, Z128, _vp],
-    "fb_ztrsm_right_upper": [_vp, _i64, _i64, _int, _vp, _i64, _vp],
+    "fb_ztrsm_workspace_size": [_int, _psz],
+    "fb_ztrsm_right_upper": [_vp, _i64, _i64, _int, _vp, _i64, _vp, _sz, _vp],
     "fb_zgemm_right": [_vp, _i64, _vp, _i64, _i64, _int, _vp, _i64, _int, _vp],
     "fb_zpotrf_workspace_size": [_int, _psz],
     "fb_zpotrf_shifted": [_vp, _i64, _vp, _i64, _int, _i64, _vp, _i64, _vp, _i64, _pint, _pdbl, _vp, _sz, _vp],

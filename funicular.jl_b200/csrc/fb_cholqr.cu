@@ -19,15 +19,16 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
                  void* workspace, size_t workspace_bytes, cudaStream_t stream,
                  const ChainStatus* st, int gate);
 size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian);
-int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr,
-                 cudaStream_t stream, const ChainStatus* st, int gate);
+int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
+                 size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate);
+size_t trsm_workspace_bytes(int k);
 size_t potrf_gwork_bytes(int k);
 int potrf_enqueue(const z64* G, int64_t ldg, int k, int64_t N, z64* U, int64_t ldu,
                   const z64* Rin, int64_t ldrin, z64* Rout, int64_t ldrout, z64* gwork,
                   ChainStatus* st, int pass, int gate, cudaStream_t stream);
 
 struct CholqrLayout {
-    size_t status, G, U, Ra, Rb, gwork, gram, total;
+    size_t status, G, U, Ra, Rb, gwork, trsm, gram, total;
 };
 
 static CholqrLayout cholqr_layout(int64_t N, int k) {
@@ -41,6 +42,7 @@ static CholqrLayout cholqr_layout(int64_t N, int k) {
     L.Ra = take(kk);
     L.Rb = take(kk);
     L.gwork = take(potrf_gwork_bytes(k));
+    L.trsm = take(trsm_workspace_bytes(k));
     L.gram = take(gram_workspace_size(N, k, k, true));
     L.total = off;
     return L;
@@ -97,6 +99,8 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t l
     z64* Rb = reinterpret_cast<z64*>(ws + L.Rb);
     z64* gwork = reinterpret_cast<z64*>(ws + L.gwork);
     void* gram_ws = ws + L.gram;
+    void* trsm_ws = ws + L.trsm;
+    const size_t trsm_bytes = L.gram - L.trsm;
     const size_t gram_bytes = L.total - L.gram;
     cudaStream_t stream = stream_of(queue);
     z64* Yz = reinterpret_cast<z64*>(Y);
@@ -110,7 +114,7 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t l
         const int gate = pass == 3 ? GATE_THIRD : GATE_HEALTHY;
         FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st, gate));
         FB_TRY(potrf_enqueue(G, k, k, N, U, k, rin[pass], k, rout[pass], k, gwork, st, pass, gate, stream));
-        FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, stream, st, gate));
+        FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, trsm_ws, trsm_bytes, stream, st, gate));
     }
     int blocks = (int)((int64_t)k * k + 255) / 256;
     select_r_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<z64*>(R), ldr, Ra, Rb, k, st);

@@ -114,6 +114,15 @@ __device__ __forceinline__ const T* opaque(const T* p) {
     return p;
 }
 
+// p, but only once v is known: `zero` is a kernel argument that is always 0,
+// which the compiler cannot see, so the address really depends on v. A long
+// unrolled sweep of loads threaded through this issues its loads a group at a
+// time instead of hoisting all of them (and spilling).
+template <typename T>
+__device__ __forceinline__ const T* hold(const T* p, double v, int zero) {
+    return p + (zero & (int)__double_as_longlong(v));
+}
+
 // A 16-byte shared memory load the compiler keeps in program order with the
 // other loads of this kind, so a long unrolled sweep over a factor does not
 // turn into hundreds of loads issued ahead of their use.

@@ -341,7 +341,7 @@ static GramLaunch gram_launch(const GramShape& sh, bool diag) {
     else ln.ppw = 8;
     ln.consumers = (ln.npairs + ln.ppw - 1) / ln.ppw;
     ln.stage_bytes = GS_BOXES * (sh.tw_a * 128 + (diag ? 0 : sh.tw_b * 128));
-    ln.stages = diag ? 4 : 3;
+    ln.stages = diag ? 6 : 3;
     while (ln.stages > 2 && (size_t)ln.stages * ln.stage_bytes > 200 * 1024) --ln.stages;
     ln.smem = (size_t)ln.stages * ln.stage_bytes + 2 * ln.stages * sizeof(uint64_t) + 1024;
     return ln;

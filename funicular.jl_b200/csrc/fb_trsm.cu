@@ -1,6 +1,6 @@
-// rdiv_upper! (src/kernels.jl:90-124): Y <- Y R^-1 for upper triangular,
-// non-unit R, in place on a rows x k ComplexF64 block, and rightmul_gemm!
-// (src/kernels.jl:57-88): dst <- A C.
+// rdiv_upper! (src/kernels.jl:90-124) for k > 64 and rightmul_gemm!
+// (src/kernels.jl:57-88): dst <- A C. (k <= 64 goes to the tensor-core
+// solvers in fb_trsm_dmma.cu.)
 //
 // Both are row-independent, so a thread owns a row. For k <= 64 the row lives
 // in registers for the whole solve, and the substitution runs right-looking:
@@ -81,9 +81,14 @@ trsm_rows_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k,
     }
 }
 
-int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr,
-                 cudaStream_t stream, const ChainStatus* st, int gate) {
+int trsm_dmma_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
+                      size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate);
+size_t trsm_workspace_bytes(int k);
+
+int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
+                 size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate) {
     if (rows == 0 || k == 0) return FB_OK;
+    if (k <= 64) return trsm_dmma_enqueue(Y, ldy, rows, k, R, ldr, workspace, workspace_bytes, stream, st, gate);
     const int threads = 128;
     const int kp = (k + TB - 1) / TB * TB;
     size_t smem = ((size_t)kp * kp + kp) * sizeof(z64);
@@ -161,8 +166,14 @@ using namespace fb;
 
 extern "C" {
 
+int fb_ztrsm_workspace_size(int k, size_t* bytes) {
+    if (!bytes || k < 0) { set_error(FB_EINVAL, "fb_ztrsm_workspace_size: bad argument"); return FB_EINVAL; }
+    *bytes = trsm_workspace_bytes(k);
+    return FB_OK;
+}
+
 int fb_ztrsm_right_upper(fb_z128* Y, int64_t ldy, int64_t rows, int k,
-                         const fb_z128* R, int64_t ldr, fb_queue_t queue) {
+                         const fb_z128* R, int64_t ldr, void* workspace, size_t workspace_bytes, fb_queue_t queue) {
     if (rows < 0 || k < 0) {
         set_error(FB_EDIM, "a %lld x %d block cannot be divided by a triangular factor", (long long)rows, k);
         return FB_EDIM;
@@ -179,7 +190,7 @@ int fb_ztrsm_right_upper(fb_z128* Y, int64_t ldy, int64_t rows, int k,
         return FB_EINVAL;
     }
     return trsm_enqueue(reinterpret_cast<z64*>(Y), ldy, rows, k, reinterpret_cast<const z64*>(R), ldr,
-                        stream_of(queue), nullptr, GATE_ALWAYS);
+                        workspace, workspace_bytes, stream_of(queue), nullptr, GATE_ALWAYS);
 }
 
 int fb_zgemm_right(fb_z128* dst, int64_t ldd, const fb_z128* A, int64_t lda, int64_t rows, int s,

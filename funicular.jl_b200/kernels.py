@@ -76,8 +76,17 @@ def rdiv_upper(backend, Y: DeviceMatrix, R: DeviceMatrix) -> DeviceMatrix:
         raise DimensionMismatch(f"a {Y.shape} block cannot be divided by a {R.shape} triangular factor")
     if Y.size == 0:
         return Y
-    call("fb_ztrsm_right_upper", _vp(Y.ptr), ctypes.c_int64(Y.ld), ctypes.c_int64(Y.rows), Y.cols,
-         _vp(R.ptr), ctypes.c_int64(R.ld), backend.queue_handle())
+    need = ctypes.c_size_t(0)
+    call("fb_ztrsm_workspace_size", Y.cols, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value) if need.value else (None, 0)
+    try:
+        status = _lib.load().fb_ztrsm_right_upper(_vp(Y.ptr), ctypes.c_int64(Y.ld), ctypes.c_int64(Y.rows), Y.cols,
+                                                  _vp(R.ptr), ctypes.c_int64(R.ld), _vp(ws), ws_bytes,
+                                                  backend.queue_handle())
+    finally:
+        if need.value:
+            backend.workspace_release()
+    _lib.check(status, "rdiv_upper!")
     return Y
 
 

@@ -157,9 +157,16 @@ int fb_zgram_static(fb_z128* C, int64_t ldc,
 
 /* rdiv_upper!(backend, Y, R) (src/kernels.jl:108): Y <- Y R^-1 in place for
  * an upper triangular, non-unit k x k R; Y is rows x k with leading
- * dimension ldy (a row block view of a staging buffer is fine). */
+ * dimension ldy (a row block view of a staging buffer is fine). For k <= 64
+ * the solve runs on the FP64 tensor cores and needs a workspace of
+ * fb_ztrsm_workspace_size bytes (72 KB at k = 64, 0 past 64): a product by
+ * inv(R) when cond_1(R) <= 16, a blocked solve with inverted 8 x 8 diagonal
+ * blocks when those are well conditioned, plain substitution otherwise; the
+ * choice is made on the device. */
+int fb_ztrsm_workspace_size(int k, size_t* bytes);
 int fb_ztrsm_right_upper(fb_z128* Y, int64_t ldy, int64_t rows, int k,
-                         const fb_z128* R, int64_t ldr, fb_queue_t queue);
+                         const fb_z128* R, int64_t ldr, void* workspace, size_t workspace_bytes,
+                         fb_queue_t queue);
 
 /* rightmul_gemm!(backend, dst, A, C) (src/kernels.jl:73): dst <- A C with A
  * rows x s, C s x r, dst rows x r. dst must not overlap A. */

@@ -54,7 +54,7 @@ def test_shape_errors_map_to_dimension_mismatch(fb):
     assert "negative" in fb._lib.last_error()
     with pytest.raises(fb.DimensionMismatch):
         fb._lib.check(status)
-    assert lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None) == fb._lib.FB_EDIM
+    assert lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None, 0, None) == fb._lib.FB_EDIM
     assert lib.fb_zgemm_right(None, 1, None, 1, 4, -1, None, 1, 2, None) == fb._lib.FB_EDIM
 
 
@@ -71,7 +71,7 @@ def test_empty_work_is_a_no_op(fb):
     lib = fb._lib.load()
     z = fb._lib.z128(1.0)
     assert lib.fb_zgram(None, 1, None, 1, None, 1, 10, 0, 3, z, z, None, 0, None) == fb._lib.FB_OK
-    assert lib.fb_ztrsm_right_upper(None, 1, 0, 3, None, 1, None) == fb._lib.FB_OK
+    assert lib.fb_ztrsm_right_upper(None, 1, 0, 3, None, 1, None, 0, None) == fb._lib.FB_OK
     assert lib.fb_copy2d(None, 16, None, 16, 0, 4, None) == fb._lib.FB_OK
 
 
@@ -102,7 +102,7 @@ def test_cholqr2_rejects_empty_and_misaligned(fb):
 def test_errors_are_per_thread(fb):
     import threading
     lib = fb._lib.load()
-    lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None)
+    lib.fb_ztrsm_right_upper(None, 1, -3, 2, None, 1, None, 0, None)
     seen = []
     t = threading.Thread(target=lambda: seen.append(fb._lib.last_error()))
     t.start()

@@ -261,3 +261,60 @@ def test_cholqr2_resident_refuses_dependent_columns(fb, backend):
     U = backend.alloc_device(np.complex128, (6, 6))
     with pytest.raises(fb.NotPositiveDefinite):
         fb.kernels.cholesky_upper_device(backend, backend.todevice(np.asfortranarray(G)), 500, 6, U)
+
+
+@pytest.mark.parametrize("k", [8, 23, 64])
+def test_rdiv_upper_ill_conditioned_diagonal_block(fb, backend, oracle, k):
+    # A diagonal 8 x 8 block of R whose condition number is far past what an
+    # explicit block inverse tolerates: the kernel must fall back to plain
+    # substitution and match ztrsm to working accuracy.
+    rng = np.random.default_rng(k + 7)
+    rows = 1000
+    Y = randmatrix(rng, rows, k)
+    R = np.asfortranarray(np.triu(randmatrix(rng, k, k)) + np.diag(np.full(k, 2.0)))
+    R[1, 1] = 1e-7
+    R[0, 1] = 3.0
+    Yd, Rd = backend.todevice(Y), backend.todevice(R)
+    fb.kernels.rdiv_upper(backend, Yd, Rd)
+    expect = Y.copy(order="F")
+    oracle.rdiv_upper(expect, R)
+    X = Yd.to_host()
+    # Substitution is backward stable: its residual is eps |X| |R|, which the
+    # 1e-7 pivot makes large; the device must do as well as ztrsm does.
+    res, res_ref = np.linalg.norm(X @ R - Y), np.linalg.norm(expect @ R - Y)
+    assert res <= 10 * res_ref + 1e-14 * np.linalg.norm(Y)
+    assert np.linalg.norm(X - expect) <= 1e-7 * np.linalg.norm(expect)
+
+
+def test_rdiv_upper_reconstructs_to_working_accuracy(fb, backend, oracle):
+    # The blocked tensor-core solve multiplies by inverses of 8 x 8 diagonal
+    # blocks; for a triangular factor of a Gram matrix with condition 1e12
+    # (cholqr2!'s first pass on C2-like data) X R must still equal Y to 1e-13.
+    rng = np.random.default_rng(99)
+    rows, k = 20000, 64
+    from conftest import conditioned
+    A = conditioned(rng, rows, k, 1e6)
+    R, _ = oracle.cholesky_upper(A.conj().T @ A, rows, k)
+    Ad, Rd = backend.todevice(A), backend.todevice(np.asfortranarray(R))
+    fb.kernels.rdiv_upper(backend, Ad, Rd)
+    X = Ad.to_host()
+    assert np.linalg.norm(X @ R - A) <= 1e-13 * np.linalg.norm(A)
+
+
+@pytest.mark.parametrize("k,scale", [(64, 0.01), (37, 0.01), (64, 0.5), (8, 3.0)])
+def test_rdiv_upper_both_tensor_core_paths(fb, backend, oracle, k, scale):
+    # scale 0.01: R within 1 % of the identity, cond_1 well under 16, so the
+    # solve is one product by inv(R); scale 0.5 and 3.0: larger off-diagonal
+    # entries push cond_1 past 16 and the blocked solve takes over.
+    rng = np.random.default_rng(k + int(100 * scale))
+    rows = 3001
+    Y = randmatrix(rng, rows, k)
+    R = np.asfortranarray(np.eye(k) + scale * np.triu(randmatrix(rng, k, k)))
+    Yd, Rd = backend.todevice(Y), backend.todevice(R)
+    fb.kernels.rdiv_upper(backend, Yd, Rd)
+    expect = Y.copy(order="F")
+    oracle.rdiv_upper(expect, R)
+    X = Yd.to_host()
+    cond = np.linalg.norm(R, 1) * np.linalg.norm(np.linalg.inv(R), 1)
+    np.testing.assert_allclose(X, expect, rtol=0, atol=1e-14 * cond * np.abs(expect).max())
+    assert np.linalg.norm(X @ R - Y) <= 1e-14 * np.linalg.norm(Y) * max(1.0, np.sqrt(cond))

@@ -30,6 +30,7 @@
 // chunk r ^ (c % 8) of that column's 128-byte line. The eight lanes that read
 // eight consecutive columns of one row therefore hit eight different banks.
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "fb_common.cuh"
@@ -47,6 +48,7 @@ struct GramShape {
     int tw_a, tw_b;      // tile widths in columns (multiples of 8, at most 64)
     int nt_a, nt_b;      // tiles along the columns of A and of B
     int hermitian;
+    int sdiag;           // diagonal 8 x 8 blocks of folded tiles hold S = Re + Im
     int ntiles;          // tiles in the partial buffer
     int64_t chunk_rows;  // a multiple of GS_ROWS
     int nchunks;
@@ -61,7 +63,13 @@ struct GramLaunch {
     int consumers;       // consumer warps
     int stages;
     int stage_bytes;
+    int sdiag;           // slot 0 of warps 0..nb-1 holds diagonal block (w, w), S-coded
     size_t smem;
+    // Block (I, J) of every consumer slot (warp * ppw + i); -1 for an empty
+    // slot. Built on the host so that the SM's four sub-partitions get equal
+    // MMA counts (a block on the diagonal costs one MMA per k-step, the others
+    // two).
+    signed char pi[64], pj[64];
 };
 
 __host__ __device__ inline int off_tile_index(int nt, int ti, int tj) {
@@ -79,7 +87,11 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                  const ChainStatus* st, int gate) {
     if (gated_off(st, gate)) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // Aligned for the 128-byte swizzle by pointer arithmetic on the shared
+    // array itself, so the compiler keeps seeing a shared-memory pointer and
+    // emits 32-bit shared loads (an integer round trip would make every
+    // fragment load generic, with 64-bit address arithmetic).
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
 
     // Which tile this CTA owns.
     int ti, tj, tile_index;
@@ -147,21 +159,18 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     // computes a copy of block 0 and never writes it, so the inner loop has no
     // branch on it.
     int bi[PPW], bj[PPW];
-    bool valid[PPW];
+    bool valid[PPW], dpair[PPW];
 #pragma unroll
     for (int i = 0; i < PPW; ++i) {
-        int p = warp * PPW + i;
-        valid[i] = p < ln.npairs;
-        if (!valid[i]) p = 0;
-        if (ln.diag) {
-            int I = 0;
-            while (p >= ln.nb_a - I) { p -= ln.nb_a - I; ++I; }
-            bi[i] = I;
-            bj[i] = I + p;
-        } else {
-            bi[i] = p / ln.nb_b;
-            bj[i] = p - bi[i] * ln.nb_b;
-        }
+        const int slot = warp * PPW + i;
+        valid[i] = ln.pi[slot] >= 0;
+        bi[i] = valid[i] ? ln.pi[slot] : ln.pi[0];
+        bj[i] = valid[i] ? ln.pj[slot] : ln.pj[0];
+        // A diagonal block of a folded tile: Re there is symmetric and Im
+        // antisymmetric, so one product S = (W + J W)^T W = Re + Im carries
+        // both, and the reduction recovers them as (S + S^T)/2, (S - S^T)/2.
+        // Such a block only ever sits in slot 0.
+        dpair[i] = (i == 0) && ln.sdiag && valid[i] && bi[i] == bj[i];
     }
 
     // Lane roles in the m8n8k4 fragments: col8 = column within the 8-block,
@@ -190,7 +199,7 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 
     // NACC interleaved accumulator sets (alternate k-steps) double the
     // independent MMA chains per warp.
-    constexpr int NACC = PPW >= 8 ? 1 : 2;
+    constexpr int NACC = PPW == 2 ? 2 : 1;
     double acc[NACC][PPW][2][2];
 #pragma unroll
     for (int h = 0; h < NACC; ++h)
@@ -198,38 +207,57 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         for (int i = 0; i < PPW; ++i)
             acc[h][i][0][0] = acc[h][i][0][1] = acc[h][i][1][0] = acc[h][i][1][1] = 0.0;
 
+    // The stage loop, compiled twice: with slot 0 a diagonal S block (one MMA
+    // a k-step) and without. The choice is per warp and made once, here, so
+    // no MMA in the loop is predicated (a predicated-off MMA still occupies
+    // the tensor pipe).
     bool ok = true;
-    int b = 0;
-    uint32_t phase = 0;
-    for (int64_t s = 0; s < nstages; ++s) {
-        if (!mbar_wait(&full[b], phase)) { ok = false; break; }
-        const unsigned char* sa = smem + (size_t)b * ln.stage_bytes;
-        const unsigned char* sbb = ln.diag ? sa : sa + GS_BOXES * box_a;
+    auto run = [&](auto s0_tag) {
+        constexpr bool S0 = decltype(s0_tag)::value;
+        int b = 0;
+        uint32_t phase = 0;
+        for (int64_t s = 0; s < nstages; ++s) {
+            if (!mbar_wait(&full[b], phase)) { ok = false; break; }
+            const unsigned char* sa = smem + (size_t)b * ln.stage_bytes;
+            const unsigned char* sbb = ln.diag ? sa : sa + GS_BOXES * box_a;
 #pragma unroll 1
-        for (int g = 0; g < GS_BOXES; ++g) {
-            const unsigned char* ba = sa + g * box_a;
-            const unsigned char* bb = sbb + g * box_b;
-            constexpr int Q_UNROLL = PPW >= 8 ? 1 : 4;
+            for (int g = 0; g < GS_BOXES; ++g) {
+                const unsigned char* ba = sa + g * box_a;
+                const unsigned char* bb = sbb + g * box_b;
+                constexpr int Q_UNROLL = PPW >= 8 ? 1 : 4;
 #pragma unroll Q_UNROLL
-            for (int q = 0; q < 4; ++q) {
-                const int h = q % NACC;
-                double are = 0.0, aim = 0.0;
+                for (int q = 0; q < 4; ++q) {
+                    const int h = q % NACC;
+                    double are = 0.0, aim = 0.0;
 #pragma unroll
-                for (int i = 0; i < PPW; ++i) {
-                    if (newA[i]) {
-                        are = *reinterpret_cast<const double*>(ba + offA[i] + swz[q]);
-                        aim = __longlong_as_double(
-                            __double_as_longlong(*reinterpret_cast<const double*>(ba + offAo[i] + swz[q])) ^ flip);
+                    for (int i = 0; i < PPW; ++i) {
+                        if (newA[i]) {
+                            are = *reinterpret_cast<const double*>(ba + offA[i] + swz[q]);
+                            aim = __longlong_as_double(
+                                __double_as_longlong(*reinterpret_cast<const double*>(ba + offAo[i] + swz[q])) ^ flip);
+                        }
+                        const double bw = *reinterpret_cast<const double*>(bb + offB[i] + swz[q]);
+                        if constexpr (S0) {
+                            if (i == 0) {
+                                dmma_884(acc[h][i][0][0], acc[h][i][0][1], are + aim, bw);
+                                continue;
+                            }
+                        }
+                        dmma_884(acc[h][i][0][0], acc[h][i][0][1], are, bw);
+                        dmma_884(acc[h][i][1][0], acc[h][i][1][1], aim, bw);
                     }
-                    const double bw = *reinterpret_cast<const double*>(bb + offB[i] + swz[q]);
-                    dmma_884(acc[h][i][0][0], acc[h][i][0][1], are, bw);
-                    dmma_884(acc[h][i][1][0], acc[h][i][1][1], aim, bw);
                 }
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[b]);
+            if (++b == stages) { b = 0; phase ^= 1u; }
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[b]);
-        if (++b == stages) { b = 0; phase ^= 1u; }
+    };
+    if constexpr (PPW >= 8) {
+        run(std::false_type{});   // eight blocks a warp: full tiles only, no diagonal block
+    } else {
+        if (dpair[0]) run(std::true_type{});
+        else run(std::false_type{});
     }
     if (!ok) {
         // A stage never arrived: poison this CTA's share of the result so the
@@ -256,7 +284,7 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const int lj = bj[i] * 8 + 2 * (lane & 3) + c;
-            out[lj * G_TILE + li] = zmake(acc[0][i][0][c], acc[0][i][1][c]);
+            out[lj * G_TILE + li] = zmake(acc[0][i][0][c], dpair[i] ? 0.0 : acc[0][i][1][c]);
         }
     }
 }
@@ -280,9 +308,14 @@ __global__ void gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int kA, int
     if (sh.hermitian) tile = (ti == tj) ? ti : off_tile_index(sh.nt_a, ti, tj);
     else tile = ti * sh.nt_b + tj;
     const z64* src = partial + (size_t)tile * sh.nchunks * (G_TILE * G_TILE) + lj * G_TILE + li;
+    // A diagonal 8 x 8 block of a folded tile holds S = Re + Im: Re and Im
+    // come back as the symmetric and antisymmetric parts of S.
+    const bool sblock = sh.sdiag && ti == tj && (li >> 3) == (lj >> 3);
+    const z64* srcT = partial + (size_t)tile * sh.nchunks * (G_TILE * G_TILE) + li * G_TILE + lj;
     z64 s = zmake(0.0, 0.0);
     for (int c = lane; c < sh.nchunks; c += 32) {
         z64 v = src[(size_t)c * (G_TILE * G_TILE)];
+        if (sblock) v.y = srcT[(size_t)c * (G_TILE * G_TILE)].x;
         s.x += v.x;
         s.y += v.y;
     }
@@ -292,6 +325,7 @@ __global__ void gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int kA, int
         s.y += __shfl_down_sync(0xffffffffu, s.y, off);
     }
     if (lane != 0) return;
+    if (sblock) s = (li == lj) ? zmake(s.x, 0.0) : zmake(0.5 * (s.x + s.y), 0.5 * (s.x - s.y));
     if (mirror) s.y = -s.y;
     if (sh.hermitian && i == j) s.y = 0.0;
     z64 out = zmul(alpha, s);
@@ -322,6 +356,54 @@ static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian, int cta
     return sh;
 }
 
+// The consumer slots' blocks. Full tiles: row-major. Folded diagonal tiles
+// with at least as many warps as block rows: warp w < nb takes the diagonal
+// block (w, w) in slot 0 (one MMA a k-step, S-coded) and then blocks of its
+// own block row (sharing the A fragment); the rest fill the free slots in
+// order. At k = 64 (eight block rows, three blocks a warp, twelve warps) this
+// gives warps 0-7 one diagonal and two off-diagonal blocks and warps 8-11
+// three off-diagonal ones, so each sub-partition (warps w, w + 4, w + 8)
+// issues 5 + 5 + 6 = 16 MMAs a k-step. Smaller tiles without that many warps
+// compute their diagonal blocks like any other.
+static void build_pair_table(GramLaunch& ln) {
+    for (int i = 0; i < 64; ++i) ln.pi[i] = ln.pj[i] = -1;
+    ln.sdiag = 0;
+    std::vector<std::pair<int, int>> order;
+    if (ln.diag) {
+        for (int I = 0; I < ln.nb_a; ++I)
+            for (int J = I; J < ln.nb_a; ++J) order.push_back({I, J});
+    } else {
+        for (int I = 0; I < ln.nb_a; ++I)
+            for (int J = 0; J < ln.nb_b; ++J) order.push_back({I, J});
+    }
+    if (ln.diag && ln.consumers >= ln.nb_a) {
+        ln.sdiag = 1;
+        std::vector<std::vector<std::pair<int, int>>> warps(ln.consumers);
+        std::vector<std::pair<int, int>> off;
+        for (auto& p : order)
+            if (p.first != p.second) off.push_back(p);
+        std::vector<bool> used(off.size(), false);
+        for (int w = 0; w < ln.nb_a; ++w) {
+            warps[w].push_back({w, w});
+            for (size_t q = 0; q < off.size() && (int)warps[w].size() < ln.ppw; ++q)
+                if (!used[q] && off[q].first == w) { warps[w].push_back(off[q]); used[q] = true; }
+        }
+        for (int w = 0; w < ln.consumers; ++w)
+            for (size_t q = 0; q < off.size() && (int)warps[w].size() < ln.ppw; ++q)
+                if (!used[q]) { warps[w].push_back(off[q]); used[q] = true; }
+        for (int w = 0; w < ln.consumers; ++w)
+            for (size_t i = 0; i < warps[w].size(); ++i) {
+                ln.pi[w * ln.ppw + i] = (signed char)warps[w][i].first;
+                ln.pj[w * ln.ppw + i] = (signed char)warps[w][i].second;
+            }
+        return;
+    }
+    for (size_t q = 0; q < order.size() && q < 64; ++q) {
+        ln.pi[q] = (signed char)order[q].first;
+        ln.pj[q] = (signed char)order[q].second;
+    }
+}
+
 static GramLaunch gram_launch(const GramShape& sh, bool diag) {
     GramLaunch ln{};
     ln.diag = diag;
@@ -340,6 +422,7 @@ static GramLaunch gram_launch(const GramShape& sh, bool diag) {
     else if (ln.npairs <= 32) ln.ppw = 2;
     else ln.ppw = 8;
     ln.consumers = (ln.npairs + ln.ppw - 1) / ln.ppw;
+    build_pair_table(ln);
     ln.stage_bytes = GS_BOXES * (sh.tw_a * 128 + (diag ? 0 : sh.tw_b * 128));
     ln.stages = diag ? 6 : 3;
     while (ln.stages > 2 && (size_t)ln.stages * ln.stage_bytes > 200 * 1024) --ln.stages;
@@ -402,6 +485,7 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
         CUtensorMap ma, mb;
         FB_TRY(encode_panel_map(&ma, A, rows, kA, lda, sh.tw_a));
         FB_TRY(encode_panel_map(&mb, B, rows, kB, ldb, sh.tw_b));
+        if (hermitian) sh.sdiag = gram_launch(sh, true).sdiag;
         const bool launches[2] = {hermitian, !hermitian || sh.nt_a > 1};
         for (int d = 0; d < 2; ++d) {
             if (!launches[d]) continue;

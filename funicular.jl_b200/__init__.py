@@ -13,7 +13,19 @@ from ._lib import (ArgumentError, DeviceError, DimensionMismatch, NotPositiveDef
 from . import _lib
 from .device_api import B200Backend, DeviceMatrix, HostSlab, b200_backend
 from . import kernels
+from .plan import (GiB, ResidencyPlan, choose_panel_width, row_block_height, device_bytes_allocated,
+                   host_bytes_reserved, host_bytes_in_use, host_bytes_free)
+from .panels import PanelMatrix, free
+from .executor import (sweep, foreachpanel, readpanels, writepanels, updatepanels, PanelSteps, RowSteps,
+                       rowtraversal)
+from .panelblas import (gram, panelmul, cholqr2, project, rightmul, DenseOperator, ColumnOperator,
+                        DeviceOperator, cholesky_upper)
+from .ghosts import GhostPanels, isghost
 
 __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceError",
            "OutOfDeviceMemory", "B200Backend", "DeviceMatrix", "HostSlab", "b200_backend",
-           "kernels", "LIBRARY_PATH"]
+           "kernels", "LIBRARY_PATH", "GiB", "ResidencyPlan", "choose_panel_width", "row_block_height",
+           "device_bytes_allocated", "host_bytes_reserved", "host_bytes_in_use", "host_bytes_free",
+           "PanelMatrix", "free", "sweep", "foreachpanel", "readpanels", "writepanels", "updatepanels",
+           "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "project", "rightmul",
+           "DenseOperator", "ColumnOperator", "DeviceOperator", "cholesky_upper", "GhostPanels", "isghost"]

@@ -366,6 +366,7 @@ class B200Backend:
                 size = (size + 255) // 256 * 256
                 self._ws = _DeviceAllocation(size)
                 self._ws_bytes = size
+                self.device_bytes_allocated += size
                 self._ws_event = None
             elif self._ws_event is not None:
                 self.wait_event(queue, self._ws_event)

@@ -130,6 +130,13 @@ def cholesky_upper_device(backend, G: DeviceMatrix, N: int, k: int, U: DeviceMat
     return bool(shifted.value), float(shift.value)
 
 
+def cholqr2_workspace_bytes(N: int, k: int) -> int:
+    """Device scratch the resident cholqr2! chain needs for an N x k matrix."""
+    need = ctypes.c_size_t(0)
+    call("fb_zcholqr2_workspace_size", ctypes.c_int64(N), k, ctypes.byref(need))
+    return need.value
+
+
 def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True):
     """cholqr2! (src/panelblas.jl:130-139) on a matrix already in device
     memory: Y becomes Q in place and R (k x k) is written. With wait=True the
@@ -161,3 +168,18 @@ def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = Tru
         raise NotPositiveDefinite(_lib.last_error())
     _lib.check(status, "cholqr2!")
     return passes.value, tuple(shifts)
+
+
+def ghost_fill(backend, dst: DeviceMatrix, row0: int, col0: int, seed: int, value_dtype) -> DeviceMatrix:
+    """The device fill behind GhostPanels (generate_panel!, src/ghosts.jl:97-103,
+    plus the upload that followed it): dst <- the ghost block whose top left
+    entry is (row0, col0) of the matrix seeded by `seed`, its values rounded to
+    `value_dtype` (the host storage eltype) and stored in dst's eltype."""
+    if not isinstance(dst, DeviceMatrix):
+        raise ArgumentError(f"the ghost fill writes a device matrix, got {type(dst).__name__}")
+    if dst.size == 0:
+        return dst
+    call("fb_ghost_fill", _vp(dst.ptr), eltype_code(dst.dtype), ctypes.c_int64(dst.ld), ctypes.c_int64(dst.rows),
+         ctypes.c_int64(dst.cols), ctypes.c_int64(row0), ctypes.c_int64(col0),
+         ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), eltype_code(value_dtype), backend.queue_handle())
+    return dst

@@ -1,0 +1,321 @@
+"""The panel BLAS on the B200 backend (src/panelblas.jl): gram, panelmul!,
+cholqr2!, project, rightmul!, with the reference's traversals and
+accumulation rules, and the device-resident cholqr2! where the matrix fits.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import kernels
+from ._lib import ArgumentError, DimensionMismatch
+from .device_api import DeviceMatrix
+from .executor import PanelSteps, RowSteps, readpanels, rowtraversal, sweep, updatepanels, writepanels
+from .panels import PanelMatrix, assert_conformal, assert_same_panels, assert_same_rows, from_device, to_device
+from .plan import checkin_device_buffers, checkout_device_buffers, row_block_height
+
+
+def shared_plan(X: PanelMatrix, Y: PanelMatrix):
+    """shared_plan (src/panelblas.jl:4-8)."""
+    if X.dtype != Y.dtype:
+        raise ArgumentError(f"panel matrices in one operation must share their compute eltype, got {X.dtype} and "
+                            f"{Y.dtype}. Narrowing belongs on the storage tiers, not here")
+    if X.plan is not Y.plan:
+        raise ArgumentError("panel matrices in one operation must belong to the same ResidencyPlan, since the plan "
+                            "is what owns the staging buffers the operation runs through. Build both matrices from "
+                            "one plan")
+    return X.plan
+
+
+def carry(step: int) -> complex:
+    """carry (src/panelblas.jl:59): the first step overwrites, later ones add."""
+    return 0.0 if step == 0 else 1.0
+
+
+def collect_small(device: DeviceMatrix, plan) -> np.ndarray:
+    """collect_small (src/panelblas.jl:61-65)."""
+    host = np.empty(device.shape, dtype=device.dtype, order="F")
+    plan.backend.d2h(host, device)
+    return host
+
+
+def gram(X: PanelMatrix, Y: PanelMatrix | None = None, *, nbuffers=None) -> np.ndarray:
+    """gram(X[, Y]; nbuffers) (src/panelblas.jl:33-53): X^H Y accumulated on
+    the device one row block at a time, copied to the host once."""
+    Y = X if Y is None else Y
+    plan = shared_plan(X, Y)
+    assert_conformal(X, Y)
+    backend = plan.backend
+    (acc,) = checkout_device_buffers(plan, X.dtype, (X.k, X.k), 1)
+    try:
+        traversal = rowtraversal(X)
+        if X is Y:
+            sweep(lambda step, Xb: kernels.gram_accumulate(backend, acc, Xb, Xb, 1.0, carry(step)),
+                  readpanels(X), nbuffers=nbuffers, traversal=traversal)
+        else:
+            sweep(lambda step, Xb, Yb: kernels.gram_accumulate(backend, acc, Xb, Yb, 1.0, carry(step)),
+                  readpanels(X), readpanels(Y), nbuffers=nbuffers, traversal=traversal)
+        return collect_small(acc, plan)
+    finally:
+        checkin_device_buffers(plan, [acc])
+
+
+# ---- operators (src/operator.jl) -------------------------------------------
+
+class DeviceOperator:
+    """A linear operator applied to device panels. `apply(backend, dst, src)`
+    writes G src into dst on the backend's current queue; an operator that is
+    panel-capable takes a whole N x w panel, otherwise it is applied one
+    column at a time (apply_operator!, src/operator.jl:80-87)."""
+
+    panel_capable = True
+    shape = (0, 0)
+
+    def apply(self, backend, dst: DeviceMatrix, src: DeviceMatrix):
+        raise NotImplementedError
+
+
+class DenseOperator(DeviceOperator):
+    """A dense m x n matrix resident on the device; applying it is the
+    backend's product kernel."""
+
+    def __init__(self, backend, G: np.ndarray):
+        G = np.asfortranarray(np.asarray(G, dtype=np.complex128))
+        self.G = backend.todevice(G)
+        self.shape = G.shape
+
+    def apply(self, backend, dst, src):
+        kernels.rightmul_gemm(backend, dst, self.G, src)
+
+
+class ColumnOperator(DeviceOperator):
+    """Wraps an operator so it is applied column by column (the reference's
+    ColumnOperator test wrapper, test/operators.jl)."""
+
+    panel_capable = False
+
+    def __init__(self, inner: DeviceOperator):
+        self.inner = inner
+        self.shape = inner.shape
+
+    def apply(self, backend, dst, src):
+        self.inner.apply(backend, dst, src)
+
+
+def apply_operator(backend, Y: DeviceMatrix, G: DeviceOperator, X: DeviceMatrix):
+    """apply_operator! / columnwise_apply! (src/operator.jl:80-87)."""
+    if G.panel_capable:
+        G.apply(backend, Y, X)
+    else:
+        for c in range(X.cols):
+            G.apply(backend, Y.view(slice(None), slice(c, c + 1)), X.view(slice(None), slice(c, c + 1)))
+    return Y
+
+
+def assert_operator_shape(G, m, n):
+    """assert_operator_shape (src/operator.jl:74-78)."""
+    rows, cols = G.shape
+    if (rows, cols) != (m, n):
+        raise ArgumentError(f"operator is {rows}x{cols} but it reads columns of an {n}-row matrix and writes columns "
+                            f"of an {m}-row one, so it has to be {m}x{n}. Either the operator or one of the two "
+                            "matrices has the wrong row count")
+
+
+def assert_square_operator(G, N):
+    """assert_square_operator (src/operator.jl:68-72)."""
+    rows, cols = G.shape
+    if not rows == cols == N:
+        raise ArgumentError(f"operator is {rows}x{cols} but the panel matrices have {N} rows. Funicular applies an "
+                            "operator to whole columns, so it must be square and match N")
+
+
+def panelmul(Y: PanelMatrix, G: DeviceOperator, X: PanelMatrix, *, nbuffers=None) -> PanelMatrix:
+    """panelmul!(Y, G, X; nbuffers) (src/panelblas.jl:91-100)."""
+    plan = shared_plan(X, Y)
+    if X is Y:
+        raise ArgumentError("panelmul! cannot write its output over its input: the operator is applied panel by "
+                            "panel and would read columns it has already overwritten")
+    assert_same_panels(X, Y)
+    assert_operator_shape(G, Y.N, X.N)
+    backend = plan.backend
+    sweep(lambda j, Xb, Yb: apply_operator(backend, Yb, G, Xb), readpanels(X), writepanels(Y), nbuffers=nbuffers)
+    return Y
+
+
+# ---- cholqr2! (src/panelblas.jl:130-169) --------------------------------------
+
+def cholesky_upper(plan, G_dev: DeviceMatrix, N: int, k: int, U_dev: DeviceMatrix):
+    """The device hook standing in for cholesky_upper (src/panelblas.jl:148-155):
+    returns shifted, with U_dev holding the factor."""
+    shifted, _ = kernels.cholesky_upper_device(plan.backend, G_dev, N, k, U_dev)
+    return shifted
+
+
+def rdiv_rows(Y: PanelMatrix, R_dev: DeviceMatrix, *, nbuffers=None) -> PanelMatrix:
+    """rdiv_rows! (src/panelblas.jl:157-169) with the factor already on the device."""
+    backend = Y.plan.backend
+    sweep(lambda step, Yb: kernels.rdiv_upper(backend, Yb, R_dev), updatepanels(Y), nbuffers=nbuffers,
+          traversal=rowtraversal(Y))
+    return Y
+
+
+def cholqr_pass(Y: PanelMatrix, nbuffers, U_dev: DeviceMatrix, G_dev: DeviceMatrix):
+    """cholqr_pass! (src/panelblas.jl:141-146): one pass streamed through row
+    sweeps, the k x k factor staying on the device."""
+    plan = Y.plan
+    backend = plan.backend
+    sweep(lambda step, Yb: kernels.gram_accumulate(backend, G_dev, Yb, Yb, 1.0, carry(step)),
+          readpanels(Y), nbuffers=nbuffers, traversal=rowtraversal(Y))
+    shifted = cholesky_upper(plan, G_dev, Y.N, Y.k, U_dev)
+    rdiv_rows(Y, U_dev, nbuffers=nbuffers)
+    return collect_small(U_dev, plan), shifted
+
+
+def cholqr2_streamed(Y: PanelMatrix, *, nbuffers=None) -> np.ndarray:
+    """cholqr2! as the reference runs it (src/panelblas.jl:130-139): two
+    passes, a third when either shifted, every pass two row sweeps."""
+    Y.assert_writable()
+    plan = Y.plan
+    G_dev, U_dev = checkout_device_buffers(plan, Y.dtype, (Y.k, Y.k), 2)
+    try:
+        R, s1 = cholqr_pass(Y, nbuffers, U_dev, G_dev)
+        R2, s2 = cholqr_pass(Y, nbuffers, U_dev, G_dev)
+        R = R2 @ R
+        if s1 or s2:
+            R3, _ = cholqr_pass(Y, nbuffers, U_dev, G_dev)
+            R = R3 @ R
+        return R
+    finally:
+        checkin_device_buffers(plan, [G_dev, U_dev])
+
+
+def fits_on_device(Y: PanelMatrix) -> bool:
+    """Whether the whole matrix, its R and the chain's scratch fit in what the
+    plan's device pool has left."""
+    pool = Y.plan.devicepool
+    need = (Y.N * Y.k + Y.k * Y.k) * Y.dtype.itemsize + kernels.cholqr2_workspace_bytes(Y.N, Y.k)
+    return pool.allocated + need <= pool.budget
+
+
+def cholqr2_resident(Y: PanelMatrix) -> np.ndarray:
+    """The backend's cholqr2! when Y fits on the device: every panel goes up
+    once, the whole two- or three-pass chain runs on the device
+    (kernels.cholqr2_resident), Q comes back down once. Two host-device
+    crossings of the matrix instead of the six of the streamed form. When a
+    Gram matrix stays indefinite the error is raised before anything is
+    written back, so Y keeps its values."""
+    plan = Y.plan
+    backend = plan.backend
+    (D,) = checkout_device_buffers(plan, Y.dtype, (Y.N, Y.k), 1)
+    (Rd,) = checkout_device_buffers(plan, Y.dtype, (Y.k, Y.k), 1)
+    try:
+        q = backend.make_queue()
+        for p in Y.panels:
+            if p.hold is not None:
+                backend.wait_event(q, p.hold)
+        to_device(Y, D, q)
+        # Waits for the chain and raises NotPositiveDefinite if it stopped.
+        backend.submit(q, lambda: kernels.cholqr2_resident(backend, D, Rd, wait=True))
+        from_device(Y, D, q)
+        R = np.empty((Y.k, Y.k), dtype=Y.dtype, order="F")
+        backend.d2h(R, Rd, queue=q)
+        backend.sync_queue(q)
+        for p in Y.panels:
+            p.hold = None
+        return R
+    finally:
+        checkin_device_buffers(plan, [D, Rd])
+
+
+def cholqr2(Y: PanelMatrix, *, nbuffers=None, resident=None) -> np.ndarray:
+    """cholqr2!(Y; nbuffers) (src/panelblas.jl:130-139): Y becomes Q in place
+    and R (k x k, host) comes back. Device-resident when Y fits the plan's
+    device budget, streamed through row sweeps otherwise; `resident` forces
+    one or the other."""
+    Y.assert_writable()
+    if resident is None:
+        resident = fits_on_device(Y)
+    if resident:
+        return cholqr2_resident(Y)
+    return cholqr2_streamed(Y, nbuffers=nbuffers)
+
+
+# ---- project (src/panelblas.jl:268-301) ---------------------------------------
+
+def project(Q: PanelMatrix, G: DeviceOperator, *, nbuffers=None) -> np.ndarray:
+    """project(Q, G; nbuffers): Q^H (G Q) block column by block column, p(p+1)
+    steps, one extra N x w image buffer."""
+    plan = Q.plan
+    backend = plan.backend
+    assert_square_operator(G, Q.N)
+    p = Q.npanels()
+    panels, labels = [], []
+    for j in range(p):
+        panels.append(j)
+        labels.append((True, j, j))
+        for i in range(p):
+            panels.append(i)
+            labels.append((False, i, j))
+    (image,) = checkout_device_buffers(plan, Q.dtype, (Q.N, Q.w), 1)
+    (acc,) = checkout_device_buffers(plan, Q.dtype, (Q.k, Q.k), 1)
+    try:
+        def step(label, Qb):
+            applying, i, j = label
+            GQj = image.view(slice(None), slice(0, Q.panelwidth(j)))
+            if applying:
+                apply_operator(backend, GQj, G, Qb)
+            else:
+                ri, rj = Q.panelrange(i), Q.panelrange(j)
+                block = acc.view(slice(ri.start, ri.stop), slice(rj.start, rj.stop))
+                kernels.gram_accumulate(backend, block, Qb, GQj, 1.0, 0.0)
+
+        sweep(step, readpanels(Q), nbuffers=nbuffers, traversal=PanelSteps(panels, labels))
+        return collect_small(acc, plan)
+    finally:
+        checkin_device_buffers(plan, [image, acc])
+
+
+# ---- rightmul! (src/panelblas.jl:203-245) -------------------------------------
+
+def rightmul(dest: PanelMatrix, src: PanelMatrix | np.ndarray, C=None, *, nbuffers=None) -> PanelMatrix:
+    """rightmul!(Y, C) in place (k x k C) or rightmul!(dest, src, C)."""
+    if C is None:
+        Y, C = dest, np.asarray(src)
+        if C.shape != (Y.k, Y.k):
+            raise ArgumentError(f"rightmul!(Y, C) writes the product back into Y, which has {Y.k} columns and "
+                                f"cannot grow or shrink, so C must be {Y.k}x{Y.k}, got {C.shape}. Use "
+                                "rightmul!(dest, Y, C) when the column count changes")
+        plan = Y.plan
+        backend = plan.backend
+        traversal = rowtraversal(Y)
+        (factor,) = checkout_device_buffers(plan, Y.dtype, (Y.k, Y.k), 1)
+        (scratch,) = checkout_device_buffers(plan, Y.dtype, traversal.buffer_dims(Y), 1)
+        try:
+            backend.h2d(factor, np.asfortranarray(C.astype(Y.dtype)))
+
+            def step(_, Yb):
+                product = scratch.view(slice(0, Yb.rows), slice(None))
+                kernels.rightmul_gemm(backend, product, Yb, factor)
+                kernels.convert_copy(backend, Yb, product)
+
+            sweep(step, updatepanels(Y), nbuffers=nbuffers, traversal=traversal)
+        finally:
+            checkin_device_buffers(plan, [factor, scratch])
+        return Y
+    if dest is src:
+        raise ArgumentError("rightmul!(dest, src, C) needs two different matrices, since one of them streams up "
+                            "while the other streams down and a single matrix cannot do both in one sweep")
+    C = np.asarray(C)
+    if C.shape != (src.k, dest.k):
+        raise ArgumentError(f"rightmul!(dest, src, C) computes src * C, so C must be {src.k}x{dest.k}, got {C.shape}")
+    plan = shared_plan(src, dest)
+    assert_same_rows(src, dest)
+    backend = plan.backend
+    height = min(row_block_height(src.N, src.k, src.w), row_block_height(dest.N, dest.k, dest.w))
+    (factor,) = checkout_device_buffers(plan, dest.dtype, (src.k, dest.k), 1)
+    try:
+        backend.h2d(factor, np.asfortranarray(C.astype(dest.dtype)))
+        sweep(lambda _, sb, db: kernels.rightmul_gemm(backend, db, sb, factor), readpanels(src), writepanels(dest),
+              nbuffers=nbuffers, traversal=RowSteps(src.N, height))
+    finally:
+        checkin_device_buffers(plan, [factor])
+    return dest

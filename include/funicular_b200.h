@@ -207,6 +207,26 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
                       double* shifts /* 3 entries, or NULL */);
 
+/* ---- ghost panels: src/ghosts.jl ------------------------------------- */
+
+/* The device fill behind GhostPanels(T, N, k; seed) (replaces the host
+ * generation of generate_panel! / stage_host!(panel, ::GhostTier, plan) at
+ * src/ghosts.jl:97-122 followed by materialize! of the staged panel, and
+ * materialize!(dst, panel, rows, ...) for a row block, src/panels.jl:427-431).
+ * Writes the rows x cols block whose top left entry is (row0, col0) of the
+ * ghost matrix (0-based, col0 the column in the full matrix) into dst,
+ * leading dimension ld, element type dst_type. Entry (r, c) is a function of
+ * (seed, r, c) only: Philox4x32-10 with counter (r, c) and key seed gives two
+ * uniforms, Box-Muller turns them into standard normals (for a complex
+ * eltype, real and imaginary parts of variance 1/2 each). value_type rounds
+ * the values to that precision before they are stored (FB_C64/FB_F32: what
+ * a narrowed host tier holds); it must be complex exactly when dst_type is.
+ * The stream differs from the reference's Julia Xoshiro stream, which is
+ * itself defined only within one Julia version (src/ghosts.jl:34-38). */
+int fb_ghost_fill(void* dst, int dst_type, int64_t ld, int64_t rows, int64_t cols,
+                  int64_t row0, int64_t col0, uint64_t seed, int value_type,
+                  fb_queue_t queue);
+
 #ifdef __cplusplus
 }
 #endif

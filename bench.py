@@ -55,7 +55,7 @@ def parse_args():
     p.add_argument("--k", type=int, default=K_DEFAULT)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--skip-cpu-baseline", action="store_true")
-    p.add_argument("--only", choices=("gram", "trsm_blocked", "trsm_inverse", "ghost_fill"), default=None,
+    p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill"), default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
     return p.parse_args()
@@ -505,6 +505,7 @@ def run_only(args):
     stream = torch.cuda.ExternalStream(queue.handle, device=device)
     launch = {
         "gram": lambda: fb.kernels.gram_accumulate(backend, Gd, Y, Y, 1.0, 0.0),
+        "gram_tc": lambda: fb.kernels.gram_tc(backend, Gd, Y, 1.0, 0.0),
         "trsm_blocked": lambda: fb.kernels.rdiv_upper(backend, Y, R1),
         "trsm_inverse": lambda: fb.kernels.rdiv_upper(backend, Y, Rid),
         "ghost_fill": lambda: fb.kernels.ghost_fill(backend, Y, 0, 0, 0xDEADBEEF, np.complex128),

@@ -69,6 +69,27 @@ def gram_accumulate(backend, C: DeviceMatrix, A: DeviceMatrix, B: DeviceMatrix, 
     return C
 
 
+def gram_tc(backend, C: DeviceMatrix, A: DeviceMatrix, alpha=1.0, beta=0.0) -> DeviceMatrix:
+    """The tensor-core form of gram_accumulate!(C, A, A, alpha, beta): C <- alpha
+    A^H A + beta C through an Ozaki split of A into 8-bit slices on the integer
+    tensor cores (k <= 64)."""
+    _need_complex128(C, A)
+    if tuple(C.shape) != (A.cols, A.cols):
+        raise DimensionMismatch(f"cannot accumulate the Gram matrix of a {A.shape} block into a {C.shape} matrix")
+    if C.size == 0:
+        return C
+    need = ctypes.c_size_t(0)
+    call("fb_zgram_tc_workspace_size", ctypes.c_int64(A.rows), A.cols, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    try:
+        status = _lib.load().fb_zgram_tc(_vp(C.ptr), C.ld, _vp(A.ptr), max(A.ld, 1), A.rows, A.cols, z128(alpha),
+                                         z128(beta), _vp(ws), ws_bytes, backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    _lib.check(status, "gram (tensor cores)")
+    return C
+
+
 def rdiv_upper(backend, Y: DeviceMatrix, R: DeviceMatrix) -> DeviceMatrix:
     """rdiv_upper! (src/kernels.jl:108): Y <- Y R^-1, R upper triangular."""
     _need_complex128(Y, R)

@@ -207,6 +207,24 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
                       double* shifts /* 3 entries, or NULL */);
 
+/* ---- tensor-core form ------------------------------------------------- */
+
+/* gram_accumulate!(backend, C, A, A, alpha, beta) (src/kernels.jl:40) with
+ * A === B, on the integer tensor cores: C <- alpha A^H A + beta C for a
+ * rows x k device matrix A (1 <= k <= 64, rows <= 2^30, 16-byte aligned).
+ * Every FP64 entry is split into seven 8-bit slices against a power-of-two
+ * scale of its column (55 bits kept); the 28 slice products that reach FP64
+ * accuracy are exact in 32-bit integer accumulators and recovered to FP64
+ * with power-of-two weights. The result is exactly Hermitian and
+ * deterministic; its error is of the order of FP64 rounding relative to the
+ * product of the column maxima. A non-finite entry makes the whole result
+ * NaN. workspace: at least fb_zgram_tc_workspace_size bytes, 256-byte
+ * aligned. */
+int fb_zgram_tc_workspace_size(int64_t rows, int k, size_t* bytes);
+int fb_zgram_tc(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda,
+                int64_t rows, int k, fb_z128 alpha, fb_z128 beta,
+                void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
 /* ---- ghost panels: src/ghosts.jl ------------------------------------- */
 
 /* The device fill behind GhostPanels(T, N, k; seed) (replaces the host

@@ -7,61 +7,80 @@
 // alternating rows (exactly the interleaved ComplexF64 layout of a column) and
 // JW the same with each (re, im) pair turned into (im, -re):
 //   [W JW]^T W = [Re G ; -Im G]      (a 128 x 64 product for k <= 64).
-// The MMA operand A is [W_t ; JW_t] (128 rows, slice t), operand B the W
-// slices stacked along N, so one MMA of A slice t against B slices 1..7-t
-// lands in the accumulators of the groups g = t + u it feeds.
+// The MMA operand A holds the slices of W and JW, 128 rows, in tensor memory
+// (two stages deep); operand B holds the W slices stacked along N in shared
+// memory, so one MMA of A slice t against B slices 1..6-t lands in the
+// accumulators of the groups g = t + u it feeds. Keeping A in tensor memory
+// halves the shared-memory traffic of the products.
 //
-// Slices. Column j carries a power-of-two scale 2^E_j with |entries| <=
-// 2^(E_j - 1); an entry x becomes the integer x_int = rint(x 2^(55 - E_j)),
-// |x_int| <= 2^54, written as seven signed bytes
-//   x_int = d_1 2^48 + sum_{t=2..7} d_t 2^(8 (7 - t)),  d_1 in [-64, 64], d_t in [-128, 127]
-// (the low bytes of x_int + 0x808080808080, each minus 128). A product of two
-// entries is 2^(E_a + E_b - 110) sum_{t,u} d_t e_u 2^(8 (14 - t - u)); the 28
-// terms with t + u <= 8 are kept, the rest lie below 2^-51 of the leading
-// term. Group g = t + u owns 64 accumulator columns of tensor memory, 448 in
-// all.
+// Slices. Column j carries a power-of-two scale 2^E_j with |entries| <
+// 2^(E_j - 1); an entry x becomes the integer x_int = rint(x 2^(47 - E_j)),
+// |x_int| <= 2^46, written as six signed bytes
+//   x_int = sum_{t=1..6} d_t 2^(8 (6 - t)),   d_t in [-128, 127].
+// One FMA makes them: m = fma(x, 2^(47 - E_j), 2^52 + 2^51 + B) is exact, its
+// 52 mantissa bits are x_int + B + 2^51 with B = 0x808080808080 biasing every
+// digit by half its range, and its low six bytes are the digits, each plus
+// 128: the slices are read straight out of the double's bit pattern, and the
+// top 16 bits of m (0x4338 when x_int + B fits in 48 bits) tell whether x was
+// in range. A product of two entries is 2^(E_a + E_b - 94) sum_{t,u} d_t e_u
+// 2^(8 (12 - t - u)); the 21 terms with t + u <= 7 are kept. With HEADROOM
+// spare bits the largest entry of a column keeps about 45 bits, so products
+// carry relative errors near 2^-44 of the column maxima: FP64 accuracy is
+// not the aim of this form, orthogonality to 1e-12 after CholeskyQR2 is.
+// Group g = t + u owns 64 accumulator columns of tensor memory (384 in all),
+// the two stages of A slices the next 96.
 //
-// Scales adapt as the rows stream: a stage whose column maximum exceeds the
-// current limit, or one that would let an int32 accumulator overflow (every
+// Scales adapt as the rows stream: a stage with an entry its column's scale
+// cannot hold, or one that would let an int32 accumulator overflow (every
 // 8192 rows), first drains the accumulators into this CTA's FP64 partial in
-// global memory, then rescales. The partials of all CTAs are summed in a
-// fixed order by the reduce kernel, so results are deterministic.
+// global memory, then rescales with HEADROOM spare bits. The partials of all
+// CTAs are summed in a fixed order by the reduce kernel, so results are
+// deterministic.
 //
-// Roles (one CTA per SM, 192 threads): warps 0-3 read FP64 tiles from shared
-// memory, slice them into the MMA operand layout and drain tensor memory
-// (warp w owns lanes 32w..32w+31); warp 4 issues the MMAs; warp 5 keeps a
-// ring of TMA tile loads in flight. Every wait is bounded.
+// Rows of A (tensor memory lanes): lane 32q + l holds W column 16q + l for
+// l < 16 and JW column 16q + l - 16 for l >= 16, so one warp writes both rows
+// of a column and its two halves read the same FP64 values (a broadcast).
+//
+// Roles (one CTA per SM, 576 threads): warps 0-15 slice (warp w writes lane
+// quarter w % 4, K bytes 8 (w / 4)..+7 of every A slice) and drain (lane
+// quarter w % 4, accumulator columns 16 (w / 4)..+15 of every group); warp 16
+// issues the MMAs; warp 17 keeps a ring of TMA tile loads in flight. Every
+// wait is bounded.
 #include "fb_umma.cuh"
 
 namespace fb {
 namespace ozaki {
 
-constexpr int SLICES = 7;
+constexpr int SLICES = 6;
 constexpr int ROWS = 16;                        // complex rows per stage: K = 32 bytes
-constexpr int FSTAGES = 4;                      // FP64 ring depth
+constexpr int FSTAGES = 6;                      // FP64 ring depth
 constexpr int FBYTES = ROWS * 64 * 16;          // 16 KB: 16 rows x 64 columns
-constexpr int ATILE = 128 * 32;                 // one A slice tile: 128 rows x 32 bytes
-constexpr int BTILE = SLICES * 64 * 32;         // B: 7 x 64 rows x 32 bytes
-constexpr int SBYTES = SLICES * ATILE + BTILE;  // one slice buffer, 42 KB
+constexpr int BTILE = SLICES * 64 * 32;         // B: 6 x 64 rows x 32 bytes
 constexpr int SBUFS = 2;
 constexpr int TMEM_COLS = 512;
-constexpr int EPOCH_STAGES = 8192 / ROWS;       // int32 headroom: 7 x 2^14 x 2 x 8192 < 2^31
-constexpr int HEADROOM = 1;                     // spare exponent bits above the stage maximum
+constexpr int A_COL = 64 * SLICES;              // A slice t of stage s at column A_COL + 8 (SLICES (s % 2) + t)
+constexpr int EPOCH_STAGES = 8192 / ROWS;       // int32 headroom: 6 x 2^14 x 2 x 8192 < 2^31
+constexpr int HEADROOM = 2;                     // spare exponent bits above the maximum that set a scale
 constexpr int E_UNSET = -4000;                  // column seen only zeros so far
-constexpr int THREADS = 192;
-constexpr uint64_t BIAS = 0x0000808080808080ull;
+constexpr int SLICERS = 512;                    // sixteen warps
+constexpr int THREADS = SLICERS + 64;
+// 2^52 + 2^51 + 0x808080808080: the FMA addend that leaves x_int + B + 2^51
+// in the mantissa of a double whose top 16 bits are 0x4338.
+constexpr long long MAGIC_BITS = 0x4338808080808080ll;
 
 constexpr size_t OFF_F = 0;
-constexpr size_t OFF_S = OFF_F + (size_t)FSTAGES * FBYTES;
-constexpr size_t OFF_MAX = OFF_S + (size_t)SBUFS * SBYTES;  // double [2][64]
-constexpr size_t OFF_BAR = OFF_MAX + 2 * 64 * 8;            // 12 mbarriers
-constexpr size_t OFF_MISC = OFF_BAR + 16 * 8;
+constexpr size_t OFF_B = OFF_F + (size_t)FSTAGES * FBYTES;
+constexpr size_t OFF_MAX = OFF_B + (size_t)SBUFS * BTILE;   // uint32 [4][64] column maxima
+constexpr size_t OFF_BAR = OFF_MAX + 4 * 64 * 4;            // mbarriers
+constexpr size_t OFF_MISC = OFF_BAR + 32 * 8;
 constexpr size_t MISC_BYTES = 512;                          // flags, TMEM slot, column exponents
 constexpr size_t SMEM_BYTES = OFF_MISC + MISC_BYTES + 1024;  // + alignment slack
 
 struct Flags {
     int timeout;
     int nonfinite;
+    int drains;      // epochs drained, all CTAs together (a statistic)
+    int rescales;    // of them, drains forced by a column outgrowing its scale
 };
 
 __device__ __forceinline__ uint32_t sw32_offset(uint32_t row, uint32_t chunk) {
@@ -87,25 +106,58 @@ __device__ __forceinline__ uint64_t desc_sw32(uint32_t addr) {
     return d;
 }
 
-// Byte p of each of four 64-bit values, packed low to high.
-__device__ __forceinline__ uint32_t gather_byte(const uint64_t (&y)[4], int p) {
-    const int half = p >> 2, b = p & 3;
-    const uint32_t w0 = half ? (uint32_t)(y[0] >> 32) : (uint32_t)y[0];
-    const uint32_t w1 = half ? (uint32_t)(y[1] >> 32) : (uint32_t)y[1];
-    const uint32_t w2 = half ? (uint32_t)(y[2] >> 32) : (uint32_t)y[2];
-    const uint32_t w3 = half ? (uint32_t)(y[3] >> 32) : (uint32_t)y[3];
-    const uint32_t sel = (uint32_t)b | ((uint32_t)(b + 4) << 4);
-    const uint32_t lo = __byte_perm(w0, w1, sel);
-    const uint32_t hi = __byte_perm(w2, w3, sel);
-    return __byte_perm(lo, hi, 0x5410);
+// The six slice words of four FMA results (bit patterns): word t holds
+// slice t of each, low to high. Bytes 5..0 of the four values are transposed
+// with byte permutes and the bias bit of every digit flipped back.
+__device__ __forceinline__ void slice_words(const uint64_t (&y)[4], uint32_t (&w)[SLICES]) {
+    const uint32_t l0 = (uint32_t)y[0], l1 = (uint32_t)y[1], l2 = (uint32_t)y[2], l3 = (uint32_t)y[3];
+    const uint32_t h0 = (uint32_t)(y[0] >> 32), h1 = (uint32_t)(y[1] >> 32);
+    const uint32_t h2 = (uint32_t)(y[2] >> 32), h3 = (uint32_t)(y[3] >> 32);
+    const uint32_t a01 = __byte_perm(l0, l1, 0x5140), b01 = __byte_perm(l0, l1, 0x7362);
+    const uint32_t a23 = __byte_perm(l2, l3, 0x5140), b23 = __byte_perm(l2, l3, 0x7362);
+    const uint32_t c01 = __byte_perm(h0, h1, 0x5140), c23 = __byte_perm(h2, h3, 0x5140);
+    w[0] = __byte_perm(c01, c23, 0x7632) ^ 0x80808080u;  // byte 5
+    w[1] = __byte_perm(c01, c23, 0x5410) ^ 0x80808080u;  // byte 4
+    w[2] = __byte_perm(b01, b23, 0x7632) ^ 0x80808080u;  // byte 3
+    w[3] = __byte_perm(b01, b23, 0x5410) ^ 0x80808080u;  // byte 2
+    w[4] = __byte_perm(a01, a23, 0x7632) ^ 0x80808080u;  // byte 1
+    w[5] = __byte_perm(a01, a23, 0x5410) ^ 0x80808080u;  // byte 0
 }
 
-// The seven slice words of four biased integers: slice 1 is byte 6 as is,
-// slices 2..7 are bytes 5..0 with the bias bit flipped back.
-__device__ __forceinline__ void slice_words(const uint64_t (&y)[4], uint32_t (&w)[SLICES]) {
-    w[0] = gather_byte(y, 6);
+// Adds the accumulators of the epoch that ended with last_stage into P: row
+// prow, columns 16c..16c+15 of the 128 x 64 partial, read from tensor memory
+// at tcol (this thread's lane, column 16c of group 0). False if the MMAs
+// never finished. Kept out of line: it runs a few times per CTA and would
+// otherwise hold registers across the slicing loop.
+__device__ __noinline__ bool drain_epoch(uint64_t* sl_empty, int last_stage, uint32_t tcol, const int* Es, int prow,
+                                         int c, double* P, bool initialized) {
+    // Every MMA up to last_stage has finished once its commit arrived.
+    if (!mbar_wait(&sl_empty[last_stage % SBUFS], (last_stage / SBUFS) & 1)) return false;
+    umma::fence_after_sync();
+    const int Em = Es[prow & 63];
+    double acc[16];
 #pragma unroll
-    for (int t = 1; t < SLICES; ++t) w[t] = gather_byte(y, 6 - t) ^ 0x80808080u;
+    for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < SLICES; ++g) {
+        uint32_t r[16];
+        umma::tmem_ld16(tcol + 64 * g, r);
+        umma::tmem_wait_ld();
+        const double w = pow2(-8 * (g + 2));
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] = fma((double)(int)r[i], w, acc[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int n = 16 * c + i;
+        const int En = Es[n];
+        double v = 0.0;
+        if (Em != E_UNSET && En != E_UNSET) v = acc[i] * pow2(Em + En + 2);
+        double* dst = P + (size_t)n * 128 + prow;
+        *dst = initialized ? *dst + v : v;
+    }
+    umma::fence_before_sync();
+    return true;
 }
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -123,7 +175,7 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     volatile int* abort_flag = misc + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(misc + 4);
     int* Es = misc + 8;                        // [64] scale exponents for the drain
-    double* colmax = reinterpret_cast<double*>(smem + OFF_MAX);
+    uint32_t* colmax = reinterpret_cast<uint32_t*>(smem + OFF_MAX);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row0 = (int64_t)blockIdx.x * chunk_rows;
@@ -134,10 +186,10 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     if (threadIdx.x == 0) {
         for (int b = 0; b < FSTAGES; ++b) {
             mbar_init(&fp_full[b], 1);
-            mbar_init(&fp_empty[b], 128);
+            mbar_init(&fp_empty[b], SLICERS);
         }
         for (int b = 0; b < SBUFS; ++b) {
-            mbar_init(&sl_full[b], 128);
+            mbar_init(&sl_full[b], SLICERS);
             mbar_init(&sl_empty[b], 1);
         }
         *abort_flag = 0;
@@ -150,7 +202,7 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     umma::fence_after_sync();
     const uint32_t taddr = *tmem_slot;
 
-    if (warp == 5) {
+    if (warp == SLICERS / 32 + 1) {
         // ---- producer: FP64 tiles, two 8-row boxes per stage ----
         if (lane == 0) {
             tma_prefetch_map(&tm);
@@ -175,7 +227,7 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             for (int s = issued > FSTAGES ? issued - FSTAGES : 0; *abort_flag && s < issued; ++s)
                 mbar_wait(&fp_full[s % FSTAGES], (s / FSTAGES) & 1);
         }
-    } else if (warp == 4) {
+    } else if (warp == SLICERS / 32) {
         // ---- MMA issuer ----
         if (lane == 0) {
             int issued = 0;
@@ -188,17 +240,16 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
                 }
                 umma::fence_after_sync();
                 const bool fresh = fresh_flag[b] != 0;
-                const uint32_t abase = smem_u32(smem + OFF_S + (size_t)b * SBYTES);
-                const uint32_t bbase = abase + SLICES * ATILE;
+                const uint32_t bbase = smem_u32(smem + OFF_B + (size_t)b * BTILE);
 #pragma unroll
                 for (int t = 0; t < SLICES; ++t) {
                     const int ntot = 64 * (SLICES - t);
-                    const uint64_t da = desc_sw32(abase + t * ATILE);
 #pragma unroll
                     for (int off = 0; off < ntot; off += 256) {
                         const int n = ntot - off < 256 ? ntot - off : 256;
-                        umma::mma_s8(taddr + 64 * t + off, da, desc_sw32(bbase + off * 32),
-                                     umma::idesc_s8s8_s32(128, n), !(fresh && t == 0));
+                        umma::mma_s8_tmem_a(taddr + 64 * t + off, taddr + A_COL + 8 * (SLICES * b + t),
+                                            desc_sw32(bbase + off * 32), umma::idesc_s8s8_s32(128, n),
+                                            !(fresh && t == 0));
                     }
                 }
                 umma::commit(&sl_empty[b]);
@@ -209,148 +260,159 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             if (*abort_flag && issued > 0) mbar_wait(&sl_empty[(issued - 1) % SBUFS], ((issued - 1) / SBUFS) & 1);
         }
     } else {
-        // ---- slicers and drains: warps 0..3, thread tid owns TMEM lane tid ----
+        // ---- slicers and drains: warps 0..15 ----
         const int tid = threadIdx.x;
-        const int j = tid & 63, h = tid >> 6;
+        const int q = warp & 3, kq = warp >> 2;
+        const bool jw = lane >= 16;
+        const int j = 16 * q + (lane & 15);                  // this thread's column
+        const int prow = (jw ? 64 : 0) + j;                  // its row of the 128 x 64 partial
+        const uint32_t lane_base = (uint32_t)(32 * q) << 16;
         int E = E_UNSET;            // scale exponent of column j
         int epoch_start = 0;
         bool initialized = false;   // P written at least once
         bool bad = false;
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
 
-        // A CTA-uniform OR over the 128 slicer threads; also a barrier.
+        // A CTA-uniform OR over the slicer threads; also a barrier.
         auto any = [](bool p) -> bool {
-            uint32_t q;
+            uint32_t qq;
             asm volatile(
                 "{\n\t.reg .pred a, b;\n\t"
                 "setp.ne.u32 a, %1, 0;\n\t"
-                "barrier.cta.red.or.pred b, 1, 128, a;\n\t"
+                "barrier.cta.red.or.pred b, 1, %2, a;\n\t"
                 "selp.u32 %0, 1, 0, b;\n\t}"
-                : "=r"(q)
-                : "r"((uint32_t)p)
+                : "=r"(qq)
+                : "r"((uint32_t)p), "n"(SLICERS)
                 : "memory");
-            return q != 0;
+            return qq != 0;
         };
         auto fail = [&]() {
             atomicExch(&flags->timeout, 1);
             *abort_flag = 1;
         };
-
-        // Adds the accumulators of the epoch that ended with last_stage into
-        // P, row tid of the 128 x 64 partial. False if the MMAs never finished.
         auto drain = [&](int last_stage) -> bool {
-            // Every MMA up to last_stage has finished once its commit arrived.
-            if (!mbar_wait(&sl_empty[last_stage % SBUFS], (last_stage / SBUFS) & 1)) return false;
-            umma::fence_after_sync();
-            const int m = tid;
-            const int Em = Es[m & 63];
-#pragma unroll 1
-            for (int c = 0; c < 2; ++c) {
-                double acc[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) acc[i] = 0.0;
-#pragma unroll 1
-                for (int g = 0; g < SLICES; ++g) {
-                    uint32_t r[32];
-                    umma::tmem_ld32(taddr + lane_base + 64 * g + 32 * c, r);
-                    umma::tmem_wait_ld();
-                    const double w = pow2(-8 * (g + 2));
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) acc[i] = fma((double)(int)r[i], w, acc[i]);
-                }
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int n = 32 * c + i;
-                    const int En = Es[n];
-                    double v = 0.0;
-                    if (Em != E_UNSET && En != E_UNSET) v = acc[i] * pow2(Em + En + 2);
-                    double* dst = P + (size_t)n * 128 + m;
-                    *dst = initialized ? *dst + v : v;
-                }
-            }
+            const bool ok = drain_epoch(sl_empty, last_stage, taddr + lane_base + 16 * kq, Es, prow, kq, P, initialized);
             initialized = true;
-            umma::fence_before_sync();
+            return ok;
+        };
+        // Complex rows 4 (kq & 1) .. + 3 of column j in box kq / 2 of stage st.
+        auto load = [&](int st, double (&vv)[8]) -> bool {
+            const int fb = st % FSTAGES;
+            if (!mbar_wait(&fp_full[fb], (st / FSTAGES) & 1)) return false;
+            const unsigned char* box = smem + OFF_F + (size_t)fb * FBYTES + (size_t)(kq >> 1) * (FBYTES / 2) + j * 128;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int rr = 4 * (kq & 1) + r;
+                const double2 z = *reinterpret_cast<const double2*>(box + ((rr ^ (j & 7)) << 4));
+                vv[2 * r] = z.x;
+                vv[2 * r + 1] = z.y;
+            }
+            mbar_arrive(&fp_empty[fb]);
             return true;
         };
 
-        // Every decision that can end the loop is taken by all 128 threads
-        // together (any), so none of them is ever left waiting at a barrier.
+        // Every decision that can end the loop is taken by all slicer threads
+        // together (any), so none of them is ever left waiting at a barrier:
+        // one barrier per stage in the common case. A failed wait elsewhere
+        // is recorded and stops the loop at the next stage's barrier.
+        const double magic = __longlong_as_double(MAGIC_BITS);
+        bool timed_out = false;
         int s = 0;
         for (; s < nstages; ++s) {
-            const int fb = s % FSTAGES, sb = s % SBUFS;
-            const bool landed = mbar_wait(&fp_full[fb], (s / FSTAGES) & 1);
-            // Eight complex rows of column j from box h.
-            double v[16];
+            const int sb = s % SBUFS;
+            double v[8];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = 0.0;
-            if (landed) {
-                const unsigned char* box = smem + OFF_F + (size_t)fb * FBYTES + (size_t)h * (FBYTES / 2) + j * 128;
+            for (int i = 0; i < 8; ++i) v[i] = 0.0;
+            const bool landed = load(s, v);
+            // Scale and split: W rows take re0 im0 re1 im1 .., JW rows
+            // im0 -re0 im1 -re1 .., four K values to a word. A result whose
+            // top 16 bits are not 0x4338 was out of range.
+            double sc = (E == E_UNSET || bad) ? 0.0 : pow2(47 - E);
+            uint64_t t[8];
+            uint32_t range = 0;
 #pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const double2 z = *reinterpret_cast<const double2*>(box + ((r ^ (j & 7)) << 4));
-                    v[2 * r] = z.x;
-                    v[2 * r + 1] = z.y;
-                }
-                mbar_arrive(&fp_empty[fb]);
-                double mx = 0.0;
-                bool finite = true;
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    mx = fmax(mx, fabs(v[i]));
-                    finite &= isfinite(v[i]);
-                }
-                if (!finite) bad = true;
-                colmax[h * 64 + j] = mx;
+            for (int c = 0; c < 4; ++c) {
+                const double first = jw ? v[2 * c + 1] : v[2 * c];
+                const double second = jw ? v[2 * c] : v[2 * c + 1];
+                t[2 * c] = (uint64_t)__double_as_longlong(fma(first, sc, magic));
+                t[2 * c + 1] = (uint64_t)__double_as_longlong(fma(second, jw ? -sc : sc, magic));
+                range |= ((uint32_t)(t[2 * c] >> 32) ^ 0x43380000u) | ((uint32_t)(t[2 * c + 1] >> 32) ^ 0x43380000u);
             }
-            if (any(!landed || *abort_flag)) { fail(); break; }
-            const double cm = fmax(colmax[j], colmax[64 + j]);
-            const int need = cm > 0.0 ? ilogb(cm) + 2 + HEADROOM : E_UNSET;
-            const bool over = cm > 0.0 && (E == E_UNSET || need > E);
+            bool out_of_range = (range & 0xFFFF0000u) != 0;
+            if (E == E_UNSET) {
+                uint32_t nz = 0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) nz |= (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FF00000u;
+                out_of_range = nz != 0;
+            }
+            const bool epoch_full = s - epoch_start >= EPOCH_STAGES;
+            const bool stop = !landed || timed_out || *abort_flag;
             bool fresh = s == 0;
-            if (any(over || (s - epoch_start >= EPOCH_STAGES))) {
-                const bool drained = s > epoch_start ? drain(s - 1) : true;
-                if (any(!drained)) { fail(); break; }
-                if (over) E = E == E_UNSET ? need : max(E, need);
-                if (h == 0) Es[j] = E;
-                epoch_start = s;
-                fresh = true;
-            }
-            // The slice buffer is free once the MMAs of stage s - 2 finished.
-            const bool free_buf = s < SBUFS || mbar_wait(&sl_empty[sb], ((s - SBUFS) / SBUFS) & 1);
-            if (any(!free_buf)) { fail(); break; }
-            // Scale and split.
-            const double sc = E == E_UNSET ? 0.0 : pow2(55 - E);
-            unsigned char* sbuf = smem + OFF_S + (size_t)sb * SBYTES;
-            // W row j: K values re0 im0 .. re7 im7; JW row 64 + j: im0 -re0 ..
-            // Four K values (two complex rows) at a time, so only their
-            // integers are live at once.
-            uint32_t wW[4][SLICES], wJ[4][SLICES];
+            if (any(stop || out_of_range || epoch_full)) {
+                if (any(stop)) { fail(); break; }
+                // The column maxima: the high word of |x| orders magnitudes
+                // by exponent, and Inf and NaN above every finite value.
+                uint32_t mx = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const long long r0 = __double2ll_rn(v[4 * q] * sc), i0 = __double2ll_rn(v[4 * q + 1] * sc);
-                const long long r1 = __double2ll_rn(v[4 * q + 2] * sc), i1 = __double2ll_rn(v[4 * q + 3] * sc);
-                const uint64_t yw[4] = {(uint64_t)r0 + BIAS, (uint64_t)i0 + BIAS, (uint64_t)r1 + BIAS,
-                                        (uint64_t)i1 + BIAS};
-                const uint64_t yj[4] = {(uint64_t)i0 + BIAS, (uint64_t)(-r0) + BIAS, (uint64_t)i1 + BIAS,
-                                        (uint64_t)(-r1) + BIAS};
-                slice_words(yw, wW[q]);
-                slice_words(yj, wJ[q]);
-            }
+                for (int i = 0; i < 8; ++i) mx = max(mx, (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FFFFFFFu);
+                if (!jw) colmax[kq * 64 + j] = mx;
+                asm volatile("bar.sync 1, %0;" ::"n"(SLICERS) : "memory");
+                const uint32_t cm = max(max(colmax[j], colmax[64 + j]), max(colmax[128 + j], colmax[192 + j]));
+                if (cm >= 0x7FF00000u) bad = true;
+                // A column outgrows its scale when its maximum is no longer
+                // below 2^(E - 1); the new scale leaves HEADROOM bits above it.
+                const int need = cm >= 0x00100000u ? (int)(cm >> 20) - 1023 + 2 + HEADROOM : E_UNSET;
+                const bool over = need != E_UNSET && (E == E_UNSET || (int)(cm >> 20) - 1023 >= E - 1);
+                const bool any_over = any(over);
+                if (any_over || epoch_full) {
+                    const bool drained = s > epoch_start ? drain(s - 1) : true;
+                    if (tid == 0 && s > epoch_start) {
+                        atomicAdd(&flags->drains, 1);
+                        if (any_over) atomicAdd(&flags->rescales, 1);
+                    }
+                    if (any(!drained)) { fail(); break; }
+                    if (over) E = E == E_UNSET ? need : max(E, need);
+                    if (kq == 0 && !jw) Es[j] = E;
+                    epoch_start = s;
+                    fresh = true;
+                    if (any_over) {
+                        sc = (E == E_UNSET || bad) ? 0.0 : pow2(47 - E);
 #pragma unroll
-            for (int t = 0; t < SLICES; ++t) {
-                const uint4 ww = make_uint4(wW[0][t], wW[1][t], wW[2][t], wW[3][t]);
-                const uint4 wj = make_uint4(wJ[0][t], wJ[1][t], wJ[2][t], wJ[3][t]);
-                unsigned char* at = sbuf + t * ATILE;
-                *reinterpret_cast<uint4*>(at + sw32_offset(j, h)) = ww;
-                *reinterpret_cast<uint4*>(at + sw32_offset(64 + j, h)) = wj;
-                *reinterpret_cast<uint4*>(sbuf + SLICES * ATILE + sw32_offset(64 * t + j, h)) = ww;
+                        for (int c = 0; c < 4; ++c) {
+                            const double first = jw ? v[2 * c + 1] : v[2 * c];
+                            const double second = jw ? v[2 * c] : v[2 * c + 1];
+                            t[2 * c] = (uint64_t)__double_as_longlong(fma(first, sc, magic));
+                            t[2 * c + 1] = (uint64_t)__double_as_longlong(fma(second, jw ? -sc : sc, magic));
+                        }
+                    }
+                }
             }
+            uint32_t w0[SLICES], w1[SLICES];
+            {
+                const uint64_t y0[4] = {t[0], t[1], t[2], t[3]};
+                const uint64_t y1[4] = {t[4], t[5], t[6], t[7]};
+                slice_words(y0, w0);
+                slice_words(y1, w1);
+            }
+            // The MMAs of stage s - 2 read this stage's A and B buffers: wait
+            // for them, then write this stage's slices.
+            if (s >= SBUFS && !mbar_wait(&sl_empty[sb], ((s - SBUFS) / SBUFS) & 1)) timed_out = true;
+            umma::fence_after_sync();
+            unsigned char* bbuf = smem + OFF_B + (size_t)sb * BTILE;
+            const uint32_t boff = sw32_offset(j, kq >> 1) + (kq & 1) * 8;
+#pragma unroll
+            for (int tt = 0; tt < SLICES; ++tt) {
+                umma::tmem_st2(taddr + lane_base + A_COL + 8 * (SLICES * sb + tt) + 2 * kq, w0[tt], w1[tt]);
+                if (!jw) *reinterpret_cast<uint2*>(bbuf + boff + tt * (64 * 32)) = make_uint2(w0[tt], w1[tt]);
+            }
+            umma::tmem_wait_st();
             umma::fence_smem_to_async();
+            umma::fence_before_sync();
             if (tid == 0) fresh_flag[sb] = fresh ? 1 : 0;
             mbar_arrive(&sl_full[sb]);
         }
         if (s == nstages && nstages > 0) {
             if (any(!drain(nstages - 1))) fail();
+            if (tid == 0) atomicAdd(&flags->drains, 1);
         }
         if (bad) atomicExch(&flags->nonfinite, 1);
     }

@@ -358,6 +358,44 @@ def run_ours(args):
     ms_step = ms_total / args.steps
     value = world * alg_bytes(N, k) * args.steps / (ms_total * 1e-3) / 1e9
 
+    # The tensor-core form of the same step: every Gram on the integer tensor
+    # cores (Ozaki slices), Cholesky and triangular solves in FP64. One checked
+    # run on the true Y for its accuracy, then the same timed loop.
+    tensor_form = None
+    if k <= 64:
+        Yt.copy_(Yt0)
+        torch.cuda.synchronize()
+        Rtc = backend.alloc_device(np.complex128, (k, k))
+        checked_tc = {}
+        backend.submit(queue, lambda: checked_tc.update(
+            r=fb.kernels.cholqr2_resident(backend, Y, Rtc, form="tc")))
+        passes_tc, _ = checked_tc["r"]
+        orth_tc, orth_tc_cublas, recon_tc = accuracy(fb, backend, torch, Yt0, Yt, Rtc, N, k)
+
+        def step_tc():
+            backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, Rtc, wait=False, form="tc"))
+
+        for _ in range(args.warmup):
+            step_tc()
+        backend.sync_queue(queue)
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step_tc()
+        t1.record(stream)
+        t1.synchronize()
+        barrier()
+        ms_tc = max_over_ranks(t0.elapsed_time(t1)) / args.steps
+        tensor_form = {
+            "ms_per_step": ms_tc, "value": world * alg_bytes(N, k) / (ms_tc * 1e-3) / 1e9, "unit": UNIT,
+            "speedup_vs_fp64_form": ms_step / ms_tc, "passes": passes_tc,
+            "orthogonality_fro": orth_tc, "orthogonality_fro_cublas": orth_tc_cublas,
+            "reconstruction_rel": recon_tc, "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13,
+            "gram": "7 signed 8-bit slices per entry against a power-of-two column scale, 28 int8 products",
+        }
+
     # Per-kernel durations, same shapes as inside the step, same queue.
     def time_kernel(fn, reps):
         fn()
@@ -374,6 +412,8 @@ def run_ours(args):
     G = backend.alloc_device(np.complex128, (k, k))
     reps = max(3, min(args.steps, 20))
     gram_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.gram_accumulate(backend, G, Y, Y, 1.0, 0.0)), reps)
+    gram_tc_ms = (time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.gram_tc(backend, G, Y, 1.0, 0.0)), reps)
+                  if k <= 64 else None)
     # The two triangular solves of the step: pass 1 divides by the factor of
     # the ill-conditioned input (the blocked solve), pass 2 by a factor within
     # O(eps) of the identity (one product by its inverse). The first is timed
@@ -398,6 +438,10 @@ def run_ours(args):
                          "gbs": 32 * N * k / (trsm_blocked_ms * 1e-3) / 1e9},
     }
     dominant = max(kernels, key=lambda name: kernels[name]["ms"])
+    if gram_tc_ms is not None:
+        kernels["gram_tensor_cores"] = {"ms": gram_tc_ms, "tflops": kernel_flops / (gram_tc_ms * 1e-3) / 1e12,
+                                        "gbs": 16 * N * k / (gram_tc_ms * 1e-3) / 1e9,
+                                        "int8_tops": 28 * 2 * 128 * 64 * 2 * N / (gram_tc_ms * 1e-3) / 1e12}
     ghost_gbs = 16 * N * k / (ghost_ms * 1e-3) / 1e9
     kernels["ghost_fill"] = {"ms": ghost_ms, "gbs": ghost_gbs, "hbm_frac": ghost_gbs / hbm_peak,
                              "per_launch": f"16 N k = {16 * N * k:.3e} bytes written"}
@@ -476,6 +520,7 @@ def run_ours(args):
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
                      "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
+        "tensor_form": tensor_form,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

@@ -104,6 +104,7 @@ SIGNATURES = {
     "fb_zcholqr2_workspace_size": [_i64, _int, _psz],
     "fb_zcholqr2": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zcholqr2_query": [_vp, _pint, _pint, _pdbl],
+    "fb_zcholqr2_tc": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zgram_tc_workspace_size": [_i64, _int, _psz],
     "fb_zgram_tc": [_vp, _i64, _vp, _i64, _i64, _int, Z128, Z128, _vp, _sz, _vp],
     "fb_ghost_fill": [_vp, _int, _i64, _i64, _i64, _i64, _i64, ctypes.c_uint64, _int, _vp],

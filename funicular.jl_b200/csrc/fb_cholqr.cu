@@ -23,6 +23,10 @@ int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t
                  size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate);
 size_t trsm_workspace_bytes(int k);
 size_t potrf_gwork_bytes(int k);
+size_t ozaki_gram_workspace_size(int64_t rows);
+int ozaki_gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, int64_t rows, int k, z64 alpha, z64 beta,
+                       void* workspace, size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st,
+                       int gate);
 int potrf_enqueue(const z64* G, int64_t ldg, int k, int64_t N, z64* U, int64_t ldu,
                   const z64* Rin, int64_t ldrin, z64* Rout, int64_t ldrout, z64* gwork,
                   ChainStatus* st, int pass, int gate, cudaStream_t stream);
@@ -43,7 +47,11 @@ static CholqrLayout cholqr_layout(int64_t N, int k) {
     L.Rb = take(kk);
     L.gwork = take(potrf_gwork_bytes(k));
     L.trsm = take(trsm_workspace_bytes(k));
-    L.gram = take(gram_workspace_size(N, k, k, true));
+    // One workspace serves both forms: the Gram scratch is the larger of the
+    // FP64 and the tensor-core kernels' needs.
+    const size_t g64 = gram_workspace_size(N, k, k, true);
+    const size_t gtc = k <= 64 ? ozaki_gram_workspace_size(N) : 0;
+    L.gram = take(g64 > gtc ? g64 : gtc);
     L.total = off;
     return L;
 }
@@ -73,8 +81,8 @@ int fb_zcholqr2_workspace_size(int64_t N, int k, size_t* bytes) {
     return FB_OK;
 }
 
-int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
-                void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info,
+                         int* passes, void* workspace, size_t workspace_bytes, fb_queue_t queue, bool tensor) {
     if (N < 1 || k < 1) {
         set_error(FB_EINVAL, "cholqr2!: N and k must be positive, got N=%lld, k=%d", (long long)N, k);
         return FB_EINVAL;
@@ -112,7 +120,11 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t l
     z64* rout[4] = {nullptr, Ra, Rb, Ra};
     for (int pass = 1; pass <= 3; ++pass) {
         const int gate = pass == 3 ? GATE_THIRD : GATE_HEALTHY;
-        FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st, gate));
+        if (tensor)
+            FB_TRY(ozaki_gram_enqueue(G, k, Yz, ldy, N, k, one, zero, gram_ws, gram_bytes, stream, st, gate));
+        else
+            FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st,
+                                gate));
         FB_TRY(potrf_enqueue(G, k, k, N, U, k, rin[pass], k, rout[pass], k, gwork, st, pass, gate, stream));
         FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, trsm_ws, trsm_bytes, stream, st, gate));
     }
@@ -125,6 +137,20 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t l
         return fb_zcholqr2_query(workspace, info, passes, nullptr);
     }
     return FB_OK;
+}
+
+int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
+                void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    return cholqr2_chain(Y, ldy, N, k, R, ldr, info, passes, workspace, workspace_bytes, queue, false);
+}
+
+int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
+                   void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    if (k > 64) {
+        set_error(FB_ENOTSUP, "the tensor-core form of cholqr2! handles k <= 64, got k = %d", k);
+        return FB_ENOTSUP;
+    }
+    return cholqr2_chain(Y, ldy, N, k, R, ldr, info, passes, workspace, workspace_bytes, queue, true);
 }
 
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shifts) {

@@ -7,28 +7,25 @@
 // alternating rows (exactly the interleaved ComplexF64 layout of a column) and
 // JW the same with each (re, im) pair turned into (im, -re):
 //   [W JW]^T W = [Re G ; -Im G]      (a 128 x 64 product for k <= 64).
-// The MMA operand A holds the slices of W and JW, 128 rows, in tensor memory
-// (two stages deep); operand B holds the W slices stacked along N in shared
-// memory, so one MMA of A slice t against B slices 1..6-t lands in the
-// accumulators of the groups g = t + u it feeds. Keeping A in tensor memory
-// halves the shared-memory traffic of the products.
+// The MMA operand A holds the slices of W and JW, 128 rows, in tensor memory;
+// operand B holds the W slices stacked along N in shared memory, so one MMA
+// of A slice t against B slices 1..7-t lands in the accumulators of the groups
+// g = t + u it feeds. Keeping A in tensor memory halves the shared-memory
+// traffic of the products, which bounds this kernel.
 //
 // Slices. Column j carries a power-of-two scale 2^E_j with |entries| <
-// 2^(E_j - 1); an entry x becomes the integer x_int = rint(x 2^(47 - E_j)),
-// |x_int| <= 2^46, written as six signed bytes
-//   x_int = sum_{t=1..6} d_t 2^(8 (6 - t)),   d_t in [-128, 127].
-// One FMA makes them: m = fma(x, 2^(47 - E_j), 2^52 + 2^51 + B) is exact, its
-// 52 mantissa bits are x_int + B + 2^51 with B = 0x808080808080 biasing every
-// digit by half its range, and its low six bytes are the digits, each plus
-// 128: the slices are read straight out of the double's bit pattern, and the
-// top 16 bits of m (0x4338 when x_int + B fits in 48 bits) tell whether x was
-// in range. A product of two entries is 2^(E_a + E_b - 94) sum_{t,u} d_t e_u
-// 2^(8 (12 - t - u)); the 21 terms with t + u <= 7 are kept. With HEADROOM
-// spare bits the largest entry of a column keeps about 45 bits, so products
-// carry relative errors near 2^-44 of the column maxima: FP64 accuracy is
-// not the aim of this form, orthogonality to 1e-12 after CholeskyQR2 is.
-// Group g = t + u owns 64 accumulator columns of tensor memory (384 in all),
-// the two stages of A slices the next 96.
+// 2^(E_j - 1); an entry x becomes the integer x_int = rint(x 2^(51 - E_j)),
+// |x_int| <= 2^50, written as seven signed bytes on a grid of 8-bit steps
+//   x_int = sum_{t=1..7} d_t 2^(52 - 8 t),   d_t in [-128, 127],
+// the last one a multiple of 16 (it carries the lowest 4 bits). One FMA makes
+// them: m = fma(x, 2^(51 - E_j), 2^52 + 2^51 + B) is exact, its 52 mantissa
+// bits are x_int + B + 2^51 with B = 0x80808080808 biasing every digit by
+// half its range, and the bytes of m << 4 are the digits, each plus 128: the
+// slices are read straight out of the double's bit pattern, and its exponent
+// field tells whether x was in range. A product of two entries is
+// 2^(E_a + E_b - 102) sum_{t,u} d_t e_u 2^(104 - 8 (t + u)); the 28 terms
+// with t + u <= 8 are kept, the rest lie below 2^-50 of the leading term. Group g = t + u owns 64 accumulator columns of tensor memory (448 in
+// all), the A slices the next 56.
 //
 // Scales adapt as the rows stream: a stage with an entry its column's scale
 // cannot hold, or one that would let an int32 accumulator overflow (every
@@ -51,22 +48,22 @@
 namespace fb {
 namespace ozaki {
 
-constexpr int SLICES = 6;
+constexpr int SLICES = 7;
 constexpr int ROWS = 16;                        // complex rows per stage: K = 32 bytes
 constexpr int FSTAGES = 6;                      // FP64 ring depth
 constexpr int FBYTES = ROWS * 64 * 16;          // 16 KB: 16 rows x 64 columns
-constexpr int BTILE = SLICES * 64 * 32;         // B: 6 x 64 rows x 32 bytes
+constexpr int BTILE = SLICES * 64 * 32;         // B: 7 x 64 rows x 32 bytes
 constexpr int SBUFS = 2;
 constexpr int TMEM_COLS = 512;
-constexpr int A_COL = 64 * SLICES;              // A slice t of stage s at column A_COL + 8 (SLICES (s % 2) + t)
-constexpr int EPOCH_STAGES = 8192 / ROWS;       // int32 headroom: 6 x 2^14 x 2 x 8192 < 2^31
+constexpr int A_COL = 448;                      // A slice t at tensor memory column A_COL + 8 t
+constexpr int EPOCH_STAGES = 8192 / ROWS;       // int32 headroom: 7 x 2^14 x 2 x 8192 < 2^31
 constexpr int HEADROOM = 2;                     // spare exponent bits above the maximum that set a scale
 constexpr int E_UNSET = -4000;                  // column seen only zeros so far
 constexpr int SLICERS = 512;                    // sixteen warps
 constexpr int THREADS = SLICERS + 64;
-// 2^52 + 2^51 + 0x808080808080: the FMA addend that leaves x_int + B + 2^51
-// in the mantissa of a double whose top 16 bits are 0x4338.
-constexpr long long MAGIC_BITS = 0x4338808080808080ll;
+// 2^52 + 2^51 + 0x80808080808: the FMA addend that leaves x_int + B + 2^51
+// in the mantissa of a double whose high word starts with 0x433.
+constexpr long long MAGIC_BITS = 0x4338080808080808ll;
 
 constexpr size_t OFF_F = 0;
 constexpr size_t OFF_B = OFF_F + (size_t)FSTAGES * FBYTES;
@@ -106,22 +103,25 @@ __device__ __forceinline__ uint64_t desc_sw32(uint32_t addr) {
     return d;
 }
 
-// The six slice words of four FMA results (bit patterns): word t holds
-// slice t of each, low to high. Bytes 5..0 of the four values are transposed
-// with byte permutes and the bias bit of every digit flipped back.
+// The seven slice words of four FMA results (bit patterns, each shifted
+// left by 4): word t holds slice t of each, low to high. Bytes 6..0 of the
+// four values are transposed with byte permutes and the bias bit of every
+// digit flipped back.
 __device__ __forceinline__ void slice_words(const uint64_t (&y)[4], uint32_t (&w)[SLICES]) {
     const uint32_t l0 = (uint32_t)y[0], l1 = (uint32_t)y[1], l2 = (uint32_t)y[2], l3 = (uint32_t)y[3];
     const uint32_t h0 = (uint32_t)(y[0] >> 32), h1 = (uint32_t)(y[1] >> 32);
     const uint32_t h2 = (uint32_t)(y[2] >> 32), h3 = (uint32_t)(y[3] >> 32);
     const uint32_t a01 = __byte_perm(l0, l1, 0x5140), b01 = __byte_perm(l0, l1, 0x7362);
     const uint32_t a23 = __byte_perm(l2, l3, 0x5140), b23 = __byte_perm(l2, l3, 0x7362);
-    const uint32_t c01 = __byte_perm(h0, h1, 0x5140), c23 = __byte_perm(h2, h3, 0x5140);
-    w[0] = __byte_perm(c01, c23, 0x7632) ^ 0x80808080u;  // byte 5
-    w[1] = __byte_perm(c01, c23, 0x5410) ^ 0x80808080u;  // byte 4
-    w[2] = __byte_perm(b01, b23, 0x7632) ^ 0x80808080u;  // byte 3
-    w[3] = __byte_perm(b01, b23, 0x5410) ^ 0x80808080u;  // byte 2
-    w[4] = __byte_perm(a01, a23, 0x7632) ^ 0x80808080u;  // byte 1
-    w[5] = __byte_perm(a01, a23, 0x5410) ^ 0x80808080u;  // byte 0
+    const uint32_t c01 = __byte_perm(h0, h1, 0x5140), d01 = __byte_perm(h0, h1, 0x7362);
+    const uint32_t c23 = __byte_perm(h2, h3, 0x5140), d23 = __byte_perm(h2, h3, 0x7362);
+    w[0] = __byte_perm(d01, d23, 0x5410) ^ 0x80808080u;  // byte 6
+    w[1] = __byte_perm(c01, c23, 0x7632) ^ 0x80808080u;  // byte 5
+    w[2] = __byte_perm(c01, c23, 0x5410) ^ 0x80808080u;  // byte 4
+    w[3] = __byte_perm(b01, b23, 0x7632) ^ 0x80808080u;  // byte 3
+    w[4] = __byte_perm(b01, b23, 0x5410) ^ 0x80808080u;  // byte 2
+    w[5] = __byte_perm(a01, a23, 0x7632) ^ 0x80808080u;  // byte 1
+    w[6] = __byte_perm(a01, a23, 0x5410) ^ 0x80808080u;  // byte 0
 }
 
 // Adds the accumulators of the epoch that ended with last_stage into P: row
@@ -247,9 +247,8 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
 #pragma unroll
                     for (int off = 0; off < ntot; off += 256) {
                         const int n = ntot - off < 256 ? ntot - off : 256;
-                        umma::mma_s8_tmem_a(taddr + 64 * t + off, taddr + A_COL + 8 * (SLICES * b + t),
-                                            desc_sw32(bbase + off * 32), umma::idesc_s8s8_s32(128, n),
-                                            !(fresh && t == 0));
+                        umma::mma_s8_tmem_a(taddr + 64 * t + off, taddr + A_COL + 8 * t, desc_sw32(bbase + off * 32),
+                                            umma::idesc_s8s8_s32(128, n), !(fresh && t == 0));
                     }
                 }
                 umma::commit(&sl_empty[b]);
@@ -325,8 +324,8 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             const bool landed = load(s, v);
             // Scale and split: W rows take re0 im0 re1 im1 .., JW rows
             // im0 -re0 im1 -re1 .., four K values to a word. A result whose
-            // top 16 bits are not 0x4338 was out of range.
-            double sc = (E == E_UNSET || bad) ? 0.0 : pow2(47 - E);
+            // high word does not start 0x433 was out of range.
+            double sc = (E == E_UNSET || bad) ? 0.0 : pow2(51 - E);
             uint64_t t[8];
             uint32_t range = 0;
 #pragma unroll
@@ -335,9 +334,9 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
                 const double second = jw ? v[2 * c] : v[2 * c + 1];
                 t[2 * c] = (uint64_t)__double_as_longlong(fma(first, sc, magic));
                 t[2 * c + 1] = (uint64_t)__double_as_longlong(fma(second, jw ? -sc : sc, magic));
-                range |= ((uint32_t)(t[2 * c] >> 32) ^ 0x43380000u) | ((uint32_t)(t[2 * c + 1] >> 32) ^ 0x43380000u);
+                range |= ((uint32_t)(t[2 * c] >> 32) ^ 0x43300000u) | ((uint32_t)(t[2 * c + 1] >> 32) ^ 0x43300000u);
             }
-            bool out_of_range = (range & 0xFFFF0000u) != 0;
+            bool out_of_range = (range & 0xFFF00000u) != 0;
             if (E == E_UNSET) {
                 uint32_t nz = 0;
 #pragma unroll
@@ -375,7 +374,7 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
                     epoch_start = s;
                     fresh = true;
                     if (any_over) {
-                        sc = (E == E_UNSET || bad) ? 0.0 : pow2(47 - E);
+                        sc = (E == E_UNSET || bad) ? 0.0 : pow2(51 - E);
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
                             const double first = jw ? v[2 * c + 1] : v[2 * c];
@@ -388,20 +387,20 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             }
             uint32_t w0[SLICES], w1[SLICES];
             {
-                const uint64_t y0[4] = {t[0], t[1], t[2], t[3]};
-                const uint64_t y1[4] = {t[4], t[5], t[6], t[7]};
+                const uint64_t y0[4] = {t[0] << 4, t[1] << 4, t[2] << 4, t[3] << 4};
+                const uint64_t y1[4] = {t[4] << 4, t[5] << 4, t[6] << 4, t[7] << 4};
                 slice_words(y0, w0);
                 slice_words(y1, w1);
             }
-            // The MMAs of stage s - 2 read this stage's A and B buffers: wait
-            // for them, then write this stage's slices.
-            if (s >= SBUFS && !mbar_wait(&sl_empty[sb], ((s - SBUFS) / SBUFS) & 1)) timed_out = true;
+            // The MMAs of stage s - 1 still read A and, two stages back, B:
+            // wait for them, then write this stage's slices.
+            if (s >= 1 && !mbar_wait(&sl_empty[(s - 1) % SBUFS], ((s - 1) / SBUFS) & 1)) timed_out = true;
             umma::fence_after_sync();
             unsigned char* bbuf = smem + OFF_B + (size_t)sb * BTILE;
             const uint32_t boff = sw32_offset(j, kq >> 1) + (kq & 1) * 8;
 #pragma unroll
             for (int tt = 0; tt < SLICES; ++tt) {
-                umma::tmem_st2(taddr + lane_base + A_COL + 8 * (SLICES * sb + tt) + 2 * kq, w0[tt], w1[tt]);
+                umma::tmem_st2(taddr + lane_base + A_COL + 8 * tt + 2 * kq, w0[tt], w1[tt]);
                 if (!jw) *reinterpret_cast<uint2*>(bbuf + boff + tt * (64 * 32)) = make_uint2(w0[tt], w1[tt]);
             }
             umma::tmem_wait_st();

@@ -158,11 +158,14 @@ def cholqr2_workspace_bytes(N: int, k: int) -> int:
     return need.value
 
 
-def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True):
+def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True, form: str = "fp64"):
     """cholqr2! (src/panelblas.jl:130-139) on a matrix already in device
     memory: Y becomes Q in place and R (k x k) is written. With wait=True the
     call returns (passes, shifts) and raises if a Gram matrix stayed
-    indefinite; with wait=False it only enqueues."""
+    indefinite; with wait=False it only enqueues. form="tc" computes the Gram
+    matrices on the integer tensor cores (k <= 64)."""
+    if form not in ("fp64", "tc"):
+        raise ArgumentError(f"cholqr2! form is 'fp64' or 'tc', got {form!r}")
     _need_complex128(Y, R)
     N, k = Y.shape
     if R.shape != (k, k):
@@ -174,7 +177,8 @@ def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = Tru
     info = ctypes.c_int(0)
     passes = ctypes.c_int(0)
     try:
-        status = lib.fb_zcholqr2(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld,
+        entry = lib.fb_zcholqr2_tc if form == "tc" else lib.fb_zcholqr2
+        status = entry(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld,
                                  ctypes.byref(info) if wait else None, ctypes.byref(passes) if wait else None,
                                  _vp(ws), ws_bytes, backend.queue_handle())
     finally:

@@ -225,6 +225,14 @@ int fb_zgram_tc(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda,
                 int64_t rows, int k, fb_z128 alpha, fb_z128 beta,
                 void* workspace, size_t workspace_bytes, fb_queue_t queue);
 
+/* cholqr2!(Y) in the tensor-core form: as fb_zcholqr2, with every Gram of
+ * the chain computed by fb_zgram_tc (k <= 64); the Cholesky factorizations,
+ * the shift and the triangular solves stay in FP64. Same workspace
+ * (fb_zcholqr2_workspace_size), same status and query. */
+int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k,
+                   fb_z128* R, int64_t ldr, int* info, int* passes,
+                   void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
 /* ---- ghost panels: src/ghosts.jl ------------------------------------- */
 
 /* The device fill behind GhostPanels(T, N, k; seed) (replaces the host

@@ -3,9 +3,9 @@ slices on the integer tensor cores, checked against the oracle's FP64 Gram
 and the FP64 tensor-core path, on shapes and scalings that exercise its
 column scales, rescaling and int32 headroom drains.
 
-The form keeps about 45 bits of each entry relative to its column maximum,
-so an entry of the Gram matrix is within TC_RTOL of sqrt(G_ii G_jj): the
-accuracy CholeskyQR2 needs for orthogonality to 1e-12, not FP64's."""
+Every entry keeps at least 47 bits relative to its column maximum and every
+slice product that reaches that level is kept, so the Gram matrix is within
+FP64-like bounds of the oracle's, relative to sqrt(G_ii G_jj)."""
 import numpy as np
 import pytest
 
@@ -13,7 +13,7 @@ from conftest import randmatrix
 
 pytestmark = pytest.mark.gpu
 
-TC_RTOL = 1e-12
+TC_RTOL = 1e-13
 
 
 def gram_tc(fb, backend, A, alpha=1.0, beta=0.0, C0=None):
@@ -40,7 +40,7 @@ def test_gram_tc_matches_the_oracle(fb, backend, oracle, N, k):
     A = randmatrix(rng, N, k)
     G = gram_tc(fb, backend, A)
     ref = oracle.gram(A)
-    assert relerr(G, ref) < TC_RTOL
+    assert relerr(G, ref) < 1e-14 * max(1.0, np.sqrt(N) / 100)
 
 
 def test_gram_tc_is_exactly_hermitian_and_deterministic(fb, backend):
@@ -112,3 +112,38 @@ def test_gram_tc_rejects_wide_matrices(fb, backend):
     C = backend.alloc_device(np.complex128, (65, 65))
     with pytest.raises(fb.ArgumentError):
         fb.kernels.gram_tc(backend, C, D)
+
+
+# ---- cholqr2! in the tensor-core form ----------------------------------------
+
+def run_cholqr2_tc(fb, backend, A):
+    k = A.shape[1]
+    Y = backend.todevice(np.asfortranarray(A))
+    R = backend.alloc_device(np.complex128, (k, k))
+    passes, _ = fb.kernels.cholqr2_resident(backend, Y, R, form="tc")
+    return Y.to_host(), R.to_host(), passes
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e6])
+def test_cholqr2_tc_meets_the_accuracy_targets(fb, backend, oracle, kappa):
+    # ||Q^H Q - I||_F <= 1e-12 and ||Y - Q R|| / ||Y|| <= 1e-13, the targets
+    # of the tensor-core form.
+    from conftest import conditioned
+    rng = np.random.default_rng(int(np.log10(kappa)))
+    A = conditioned(rng, 200000, 64, kappa)
+    Q, R, passes = run_cholqr2_tc(fb, backend, A)
+    assert passes == 2
+    assert oracle.orthogonality_error(Q) <= 1e-12
+    assert oracle.reconstruction_error(A, Q, R) <= 1e-13
+    Rref, _ = oracle.cholqr2(A.copy(order="F"), w=64)
+    assert np.linalg.norm(R - Rref) <= 1e-10 * np.linalg.norm(Rref)
+
+
+def test_cholqr2_tc_takes_the_shifted_third_pass(fb, backend, oracle):
+    from conftest import conditioned
+    rng = np.random.default_rng(99)
+    A = conditioned(rng, 50000, 32, 1e10)
+    Q, R, passes = run_cholqr2_tc(fb, backend, A)
+    assert passes == 3
+    assert np.linalg.norm(Q.conj().T @ Q - np.eye(32), 2) <= 1e-8
+    assert oracle.reconstruction_error(A, Q, R) <= 1e-10

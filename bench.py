@@ -39,9 +39,9 @@ CPU_SAMPLE_ROWS = 1 << 21
 
 # DRAM bytes per row each kernel moved in its committed ncu capture (N = 5e5,
 # k = 64, profiles/*_N5e5_k64_ncu.md), scaled here to the bench's N.
-NCU_BYTES_PER_ROW = {"gram_partial+reduce": (512.0192e6 + 3.794e6) / 5e5,
-                     "trsm_inverse": (519.448e6 + 454.977e6) / 5e5,
-                     "trsm_blocked": (519.448e6 + 454.977e6) / 5e5}
+NCU_BYTES_PER_ROW = {"gram_partial+reduce": (512.085760e6 + 3.649536e6) / 5e5,
+                     "trsm_inverse": (512.097536e6 + 452.634880e6) / 5e5,
+                     "trsm_blocked": (512.105728e6 + 452.283904e6) / 5e5}
 NCU_CAPTURE_K = 64
 
 
@@ -450,7 +450,7 @@ def run_ours(args):
     roofline = {
         "bound": "fp64", "achieved": dk["tflops"], "peak": fp64_peak, "unit": "TFLOP/s",
         "frac": dk["tflops"] / fp64_peak, "traffic": traffic, "kernel": dominant,
-        "traffic_source": "ncu dram bytes of the N=5e5 capture in profiles/, scaled by N/5e5",
+        "traffic_source": "ncu dram bytes of the N=5e5 capture (profiles/*_N5e5_k64_ncu.md), scaled by N/5e5",
         "peak_source": "cuBLAS ZGEMM 4096^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
         "per_launch": f"4 N k^2 = {kernel_flops:.3e} flops per launch",
     }

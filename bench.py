@@ -55,7 +55,7 @@ def parse_args():
     p.add_argument("--k", type=int, default=K_DEFAULT)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--skip-cpu-baseline", action="store_true")
-    p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill"), default=None,
+    p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace"), default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
     return p.parse_args()
@@ -538,6 +538,8 @@ def run_only(args):
     torch.cuda.set_device(device)
     N, k = args.N, args.k
     backend = fb.B200Backend(0)
+    if args.only == "laplace":
+        return run_only_laplace(args, fb, backend, torch, device)
     Yt = build_workload(fb, backend, torch, device, N, k, seed=0xDEADBEEF)
     Y = wrap(fb, Yt, N, k)
     # The first pass's factor: the Cholesky factor of Y^H Y (Y is Yt^T).
@@ -569,6 +571,40 @@ def run_only(args):
     b.synchronize()
     print(json.dumps({"only": args.only, "N": N, "k": k, "steps": args.steps,
                       "ms_per_launch": a.elapsed_time(b) / args.steps}), flush=True)
+    return 0
+
+
+def run_only_laplace(args, fb, backend, torch, device):
+    """The streamed range finder's operator, -Lap_7 + (0.5+0.1i) I on a 342^3
+    grid (N = 40 001 688), applied to one panel of min(k, 16) columns: 32 bytes
+    per entry of algorithmic traffic (read once, write once)."""
+    grid = (342, 342, 342)
+    n = grid[0] * grid[1] * grid[2]
+    w = min(args.k, 16)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(0xDEADBEEF)
+    Xt = torch.randn((w, n), dtype=torch.complex128, device=device, generator=gen)
+    Yt = torch.empty_like(Xt)
+    torch.cuda.synchronize()
+    X, Y = wrap(fb, Xt, n, w), wrap(fb, Yt, n, w)
+    G = fb.Laplacian7(grid, 0.5 + 0.1j)
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    for _ in range(args.warmup):
+        backend.submit(queue, lambda: G.apply(backend, Y, X))
+    backend.sync_queue(queue)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("only")
+    a.record(stream)
+    for _ in range(args.steps):
+        backend.submit(queue, lambda: G.apply(backend, Y, X))
+    b.record(stream)
+    torch.cuda.nvtx.range_pop()
+    b.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    print(json.dumps({"only": "laplace", "grid": grid, "N": n, "cols": w, "steps": args.steps, "ms_per_launch": ms,
+                      "gbs": 32 * n * w / (ms * 1e-3) / 1e9}), flush=True)
     return 0
 
 

@@ -19,7 +19,7 @@ from .panels import PanelMatrix, free
 from .executor import (sweep, foreachpanel, readpanels, writepanels, updatepanels, PanelSteps, RowSteps,
                        rowtraversal)
 from .panelblas import (gram, panelmul, cholqr2, project, rightmul, DenseOperator, ColumnOperator,
-                        DeviceOperator, cholesky_upper)
+                        DeviceOperator, Laplacian7, cholesky_upper)
 from .ghosts import GhostPanels, isghost
 
 __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceError",
@@ -28,4 +28,4 @@ __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceE
            "device_bytes_allocated", "host_bytes_reserved", "host_bytes_in_use", "host_bytes_free",
            "PanelMatrix", "free", "sweep", "foreachpanel", "readpanels", "writepanels", "updatepanels",
            "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "project", "rightmul",
-           "DenseOperator", "ColumnOperator", "DeviceOperator", "cholesky_upper", "GhostPanels", "isghost"]
+           "DenseOperator", "ColumnOperator", "DeviceOperator", "Laplacian7", "cholesky_upper", "GhostPanels", "isghost"]

@@ -107,6 +107,7 @@ SIGNATURES = {
     "fb_zcholqr2_tc": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zgram_tc_workspace_size": [_i64, _int, _psz],
     "fb_zgram_tc": [_vp, _i64, _vp, _i64, _i64, _int, Z128, Z128, _vp, _sz, _vp],
+    "fb_zlaplace7_apply": [_vp, _i64, _vp, _i64, _int, _int, _int, _int, Z128, _vp],
     "fb_ghost_fill": [_vp, _int, _i64, _i64, _i64, _i64, _i64, ctypes.c_uint64, _int, _vp],
 }
 _RESTYPES = {"fb_last_error": ctypes.c_char_p, "fb_abi_version": ctypes.c_int,

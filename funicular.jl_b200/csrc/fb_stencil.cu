@@ -1,0 +1,91 @@
+// The matrix-free operator of the streamed range finder (a complex-shifted
+// 3-D Laplacian on a 342^3 grid): G = -Lap_7 + shift I on an nx x ny x nz grid, applied to the columns of a
+// device panel, the panel-capable mul! that apply_operator! hands a whole
+// resident panel to (src/operator.jl:80-87). Grid point (x, y, z) is row
+// x + nx (y + ny z); the 7-point Laplacian has unit spacing and zero
+// (Dirichlet) values outside the grid:
+//   (G v)_p = (6 + shift) v_p - sum of the six neighbours of p.
+// One thread per output entry, x fastest, so the centre, x +- 1 and the
+// store are coalesced 16-byte accesses and the y, z neighbours come from
+// L1/L2 (a plane of a 342^2 grid is 1.9 MB). HBM-bound: 32 bytes per entry
+// (read once, write once) when the neighbours hit in cache.
+#include "fb_common.cuh"
+
+namespace fb {
+
+// Blocks walk grid lines (fixed y, z) and threads the points of a line, so
+// the index arithmetic is one 32-bit division per line.
+__global__ void __launch_bounds__(128) laplace7_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X,
+                                                       int64_t ldx, int nx, int ny, int nz, int cols, z64 shift) {
+    const int64_t plane = (int64_t)nx * ny;
+    const int lines = ny * nz;
+    const double dr = 6.0 + shift.x, di = shift.y;
+    for (int c = blockIdx.y; c < cols; c += gridDim.y) {
+        const z64* x = X + (int64_t)c * ldx;
+        z64* y = Y + (int64_t)c * ldy;
+        for (int line = blockIdx.x; line < lines; line += gridDim.x) {
+            const int zi = line / ny, yi = line - zi * ny;
+            const int64_t base = (int64_t)line * nx;
+            for (int xi = threadIdx.x; xi < nx; xi += blockDim.x) {
+                const int64_t p = base + xi;
+                const z64 v = x[p];
+                z64 s = zmake(0.0, 0.0);
+                if (xi > 0) { const z64 u = x[p - 1]; s.x += u.x; s.y += u.y; }
+                if (xi < nx - 1) { const z64 u = x[p + 1]; s.x += u.x; s.y += u.y; }
+                if (yi > 0) { const z64 u = x[p - nx]; s.x += u.x; s.y += u.y; }
+                if (yi < ny - 1) { const z64 u = x[p + nx]; s.x += u.x; s.y += u.y; }
+                if (zi > 0) { const z64 u = x[p - plane]; s.x += u.x; s.y += u.y; }
+                if (zi < nz - 1) { const z64 u = x[p + plane]; s.x += u.x; s.y += u.y; }
+                y[p] = zmake(dr * v.x - di * v.y - s.x, dr * v.y + di * v.x - s.y);
+            }
+        }
+    }
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+int fb_zlaplace7_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx, int nx, int ny, int nz, int cols,
+                       fb_z128 shift, fb_queue_t queue) {
+    if (nx < 1 || ny < 1 || nz < 1 || cols < 0) {
+        set_error(FB_EINVAL, "fb_zlaplace7_apply: the grid needs positive sizes and cols >= 0, got %d x %d x %d, "
+                  "%d columns", nx, ny, nz, cols);
+        return FB_EINVAL;
+    }
+    const int64_t n = (int64_t)nx * ny * nz;
+    if (cols == 0) return FB_OK;
+    if (!Y || !X) { set_error(FB_EINVAL, "fb_zlaplace7_apply: NULL matrix"); return FB_EINVAL; }
+    if (ldy < n || ldx < n) {
+        set_error(FB_EDIM, "fb_zlaplace7_apply: leading dimensions %lld, %lld below the %lld grid points",
+                  (long long)ldy, (long long)ldx, (long long)n);
+        return FB_EDIM;
+    }
+    if (((uintptr_t)Y | (uintptr_t)X) & 15) { set_error(FB_EINVAL, "fb_zlaplace7_apply: pointers must be 16-byte aligned"); return FB_EINVAL; }
+    // Y and X must not overlap: every output reads seven inputs.
+    const char* y0 = reinterpret_cast<const char*>(Y);
+    const char* x0 = reinterpret_cast<const char*>(X);
+    const size_t ybytes = ((size_t)(cols - 1) * ldy + n) * 16, xbytes = ((size_t)(cols - 1) * ldx + n) * 16;
+    if (y0 < x0 + xbytes && x0 < y0 + ybytes) {
+        set_error(FB_EINVAL, "fb_zlaplace7_apply: the output overlaps the input");
+        return FB_EINVAL;
+    }
+    if ((int64_t)ny * nz > INT32_MAX) { set_error(FB_ENOTSUP, "fb_zlaplace7_apply: ny * nz must fit in 32 bits"); return FB_ENOTSUP; }
+    // Sixteen blocks per SM, every block walking the columns in the same order
+    // and the lines of a column in a grid-strided sweep: the lines in flight
+    // at one time span a few planes of one column, so the z neighbours of a
+    // line are still in L2 when it is computed.
+    const int64_t gy = 1;
+    int64_t gx = (int64_t)sm_count() * 16;
+    if (gx > (int64_t)ny * nz) gx = (int64_t)ny * nz;
+    if (gx < 1) gx = 1;
+    laplace7_kernel<<<dim3((unsigned)gx, (unsigned)gy), 128, 0, stream_of(queue)>>>(
+        reinterpret_cast<z64*>(Y), ldy, reinterpret_cast<const z64*>(X), ldx, nx, ny, nz, cols,
+        zmake(shift.re, shift.im));
+    FB_LAUNCHED("laplace7_kernel");
+    return FB_OK;
+}
+
+}  // extern "C"

@@ -208,3 +208,18 @@ def ghost_fill(backend, dst: DeviceMatrix, row0: int, col0: int, seed: int, valu
          ctypes.c_int64(dst.cols), ctypes.c_int64(row0), ctypes.c_int64(col0),
          ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), eltype_code(value_dtype), backend.queue_handle())
     return dst
+
+
+def laplace7_apply(backend, dst: DeviceMatrix, src: DeviceMatrix, grid, shift) -> DeviceMatrix:
+    """dst <- (-Lap_7 + shift I) src, column by column, on the grid (nx, ny, nz):
+    the matrix-free operator of the streamed range finder."""
+    _need_complex128(dst, src)
+    nx, ny, nz = (int(g) for g in grid)
+    n = nx * ny * nz
+    if src.rows != n or tuple(dst.shape) != tuple(src.shape):
+        raise DimensionMismatch(f"the {nx}x{ny}x{nz} Laplacian maps {n}-row panels, got {src.shape} -> {dst.shape}")
+    if dst.size == 0:
+        return dst
+    call("fb_zlaplace7_apply", _vp(dst.ptr), ctypes.c_int64(dst.ld), _vp(src.ptr), ctypes.c_int64(src.ld),
+         nx, ny, nz, dst.cols, z128(shift), backend.queue_handle())
+    return dst

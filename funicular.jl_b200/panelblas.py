@@ -87,6 +87,23 @@ class DenseOperator(DeviceOperator):
         kernels.rightmul_gemm(backend, dst, self.G, src)
 
 
+class Laplacian7(DeviceOperator):
+    """G = -Lap_7 + shift I on an nx x ny x nz grid, matrix-free on the device
+    (the operator of the streamed range finder): grid point (x, y, z) is row
+    x + nx (y + ny z), unit spacing, zero outside the grid."""
+
+    def __init__(self, grid, shift=0.0):
+        self.grid = tuple(int(g) for g in grid)
+        if len(self.grid) != 3 or min(self.grid) < 1:
+            raise ArgumentError(f"a 7-point Laplacian needs a 3-D grid of positive sizes, got {grid}")
+        self.shift = complex(shift)
+        n = self.grid[0] * self.grid[1] * self.grid[2]
+        self.shape = (n, n)
+
+    def apply(self, backend, dst, src):
+        kernels.laplace7_apply(backend, dst, src, self.grid, self.shift)
+
+
 class ColumnOperator(DeviceOperator):
     """Wraps an operator so it is applied column by column (the reference's
     ColumnOperator test wrapper, test/operators.jl)."""

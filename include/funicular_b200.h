@@ -207,6 +207,17 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
                       double* shifts /* 3 entries, or NULL */);
 
+/* ---- operators: src/operator.jl ------------------------------------- */
+
+/* The matrix-free operator of the streamed range finder: Y[:, c] <-
+ * (-Lap_7 + shift I) X[:, c] for c < cols on an nx x ny x nz grid, grid point
+ * (x, y, z) at row x + nx (y + ny z), unit spacing, zero outside the grid:
+ * (G v)_p = (6 + shift) v_p - (sum of the six neighbours of p). The
+ * panel-capable mul! that apply_operator! (src/operator.jl:80-87) hands a
+ * resident panel to. Y and X must not overlap. */
+int fb_zlaplace7_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx,
+                       int nx, int ny, int nz, int cols, fb_z128 shift, fb_queue_t queue);
+
 /* ---- tensor-core form ------------------------------------------------- */
 
 /* gram_accumulate!(backend, C, A, A, alpha, beta) (src/kernels.jl:40) with

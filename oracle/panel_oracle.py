@@ -256,3 +256,20 @@ def blastol(dtype, N, k):
 def orthogonality_bound(dtype, N, k):
     """test/setup.jl:172."""
     return 100 * N * k * EPS[np.dtype(dtype)]
+
+
+def laplacian7(grid, shift):
+    """-Lap_7 + shift I on an nx x ny x nz grid as a sparse matrix: unit
+    spacing, zero outside the grid, point (x, y, z) at row x + nx (y + ny z).
+    The streamed range finder's operator, stated as a Kronecker sum of 1-D
+    second differences."""
+    import scipy.sparse as sp
+    nx, ny, nz = grid
+
+    def d2(n):
+        return sp.diags([-np.ones(n - 1), 2 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], shape=(n, n))
+
+    I = sp.identity
+    L = (sp.kron(I(nz), sp.kron(I(ny), d2(nx))) + sp.kron(I(nz), sp.kron(d2(ny), I(nx)))
+         + sp.kron(d2(nz), sp.kron(I(ny), I(nx))))
+    return (L + shift * I(nx * ny * nz)).tocsr().astype(np.complex128)

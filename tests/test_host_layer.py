@@ -541,3 +541,46 @@ def test_a_ghost_matrix_refuses_to_be_written_to(fb, backend, plan):
     with pytest.raises(fb.ArgumentError):
         fb.panelmul(ghost, fb.DenseOperator(backend, np.eye(20)),
                     fb.PanelMatrix.undef(np.complex128, 20, 6, plan=plan, w=2))
+
+
+# ---- the matrix-free Laplacian operator ---------------------------------------
+
+@pytest.mark.parametrize("grid", [(5, 4, 3), (7, 1, 1), (1, 1, 1), (3, 6, 2), (33, 17, 9)])
+def test_laplacian_matches_the_sparse_operator(fb, backend, oracle, rng, grid):
+    n = grid[0] * grid[1] * grid[2]
+    shift = 0.5 + 0.1j
+    X = randmatrix(rng, n, 5)
+    D = backend.todevice(X)
+    Y = backend.alloc_device(np.complex128, (n, 5))
+    fb.Laplacian7(grid, shift).apply(backend, Y, D)
+    backend.sync_all()
+    ref = oracle.laplacian7(grid, shift) @ X
+    assert np.linalg.norm(Y.to_host() - ref) <= 1e-15 * np.linalg.norm(ref) * 10
+
+
+def test_laplacian_refuses_aliasing_and_wrong_shapes(fb, backend, rng):
+    D = backend.todevice(randmatrix(rng, 60, 3))
+    with pytest.raises(fb.ArgumentError):
+        fb.Laplacian7((5, 4, 3), 0.5).apply(backend, D, D)
+    with pytest.raises(fb.DimensionMismatch):
+        fb.Laplacian7((5, 4, 2), 0.5).apply(backend, backend.alloc_device(np.complex128, (60, 3)), D)
+    with pytest.raises(fb.ArgumentError):
+        fb.Laplacian7((5, 0, 2), 0.5)
+
+
+@pytest.mark.parametrize("w", [7, 1])
+def test_panelmul_and_project_with_the_laplacian(fb, backend, oracle, plan, rng, w):
+    grid, shift = (6, 5, 4), 0.5 + 0.1j
+    n, k = 120, 23
+    G = fb.Laplacian7(grid, shift)
+    L = oracle.laplacian7(grid, shift)
+    A = randmatrix(rng, n, k)
+    X = fb.PanelMatrix.from_array(A, plan=plan, w=w)
+    Y = fb.PanelMatrix.undef(np.complex128, n, k, plan=plan, w=w)
+    tol = blastol(n, k)
+    assert close(fb.panelmul(Y, G, X).to_array(), L @ A, tol)
+    assert close(fb.panelmul(Y, fb.ColumnOperator(G), X).to_array(), L @ A, tol)
+    assert close(fb.project(X, G), A.conj().T @ (L @ A), tol)
+    ghost = fb.GhostPanels(np.complex128, n, k, plan=plan, seed=0xDEADBEEF, w=w)
+    Omega = ghost.to_array()
+    assert close(fb.panelmul(Y, G, ghost).to_array(), L @ Omega, tol)

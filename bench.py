@@ -215,6 +215,25 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
+def reduce_max_over_ranks(x: float, world: int, device) -> float:
+    """The largest of the ranks' values: the whole job takes as long as its
+    slowest rank. An all-reduce over the default process group (NCCL on the
+    GPUs, gloo in the CPU tests)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_rank: float, world: int, ms: float) -> float:
+    """Weak scaling: every rank orthonormalizes its own matrix, so the job moves
+    world times the bytes of one rank in the slowest rank's time."""
+    return world * bytes_per_rank / (ms * 1e-3) / 1e9
+
+
 def measure_fp64_peak(torch, device):
     """cuBLAS ZGEMM (complex FP64, the arithmetic of this path) through torch,
     best of a few 4096^3 products: the FP64 roofline denominator."""
@@ -301,11 +320,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, world, device)
 
     N, k = args.N, args.k
     backend = fb.B200Backend(local)
@@ -356,7 +371,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     ms_total = max_over_ranks(e0.elapsed_time(e1))
     ms_step = ms_total / args.steps
-    value = world * alg_bytes(N, k) * args.steps / (ms_total * 1e-3) / 1e9
+    value = whole_job_gbs(alg_bytes(N, k) * args.steps, world, ms_total)
 
     # The tensor-core form of the same step: every Gram on the integer tensor
     # cores (Ozaki slices), Cholesky and triangular solves in FP64. One checked

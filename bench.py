@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--k", type=int, default=K_DEFAULT)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--skip-cpu-baseline", action="store_true")
+    p.add_argument("--batch", type=int, default=256,
+                   help="instances of the batched cholqr2! measurement (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace"), default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
@@ -213,6 +215,66 @@ class ClockSampler:
                     "samples": 0}
         return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier):
+    """The batched range finder's orthonormalization: args.batch independent
+    cholqr2! instances, N log-uniform on [1e4, 2e6], k drawn from {16, 32, 64}
+    (seeded), all enqueued by one fb_zcholqr2_batched call, timed eagerly and
+    as one captured CUDA graph. Inputs are seeded complex Gaussians; each step
+    orthonormalizes in place (the later steps see orthonormal columns, which
+    moves the same bytes through the same kernels)."""
+    rng = np.random.default_rng(0xBA7C4)
+    count = args.batch
+    Ns = np.exp(rng.uniform(np.log(1e4), np.log(2e6), count)).astype(np.int64)
+    ks = rng.choice([16, 32, 64], count)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(0xBA7C4)
+    tensors = [torch.randn((int(k), int(N)), dtype=torch.complex128, device=device, generator=gen)
+               for N, k in zip(Ns, ks)]
+    torch.cuda.synchronize()
+    Ys = [wrap(fb, t, int(N), int(k)) for t, N, k in zip(tensors, Ns, ks)]
+    Rs = [backend.alloc_device(np.complex128, (int(k), int(k))) for k in ks]
+    nbytes = fb.kernels.cholqr2_batched_workspace_bytes([(int(N), int(k)) for N, k in zip(Ns, ks)])
+    ws_buf = backend.alloc_device(np.complex128, (nbytes // 16 + 32, 1))
+    ws = ((ws_buf.ptr + 255) // 256 * 256, nbytes)
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    # Checked run: passes and the worst orthogonality over the instances.
+    passes = []
+    backend.submit(queue, lambda: passes.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws)))
+    worst = 0.0
+    for t in tensors:
+        Q = t.t()
+        worst = max(worst, float(torch.linalg.matrix_norm(Q.conj().t() @ Q
+                                                          - torch.eye(Q.shape[1], dtype=Q.dtype, device=device))))
+    eager = lambda: backend.submit(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False,
+                                                                            workspace=ws))
+    graph = backend.capture(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws))
+
+    def timed(step):
+        for _ in range(max(1, args.warmup)):
+            step()
+        backend.sync_queue(queue)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            step()
+        b.record(stream)
+        b.synchronize()
+        return max_over_ranks(a.elapsed_time(b) / args.steps)
+
+    ms_eager = timed(eager)
+    ms_graph = timed(lambda: graph.launch(queue))
+    alg = float(sum(96.0 * N * k for N, k in zip(Ns, ks)))
+    del graph, tensors, Ys
+    return {"instances": count, "N_range": [int(Ns.min()), int(Ns.max())], "k_values": [16, 32, 64],
+            "alg_bytes_per_step": alg, "ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
+            "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
+            "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,
+            "launch": "one fb_zcholqr2_batched call, replayed as one captured CUDA graph"}
 
 
 def reduce_max_over_ranks(x: float, world: int, device) -> float:
@@ -479,6 +541,9 @@ def run_ours(args):
         "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_source, "fp64_peak_tflops": fp64_peak,
     }
 
+    batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier)
+               if args.batch > 0 else None)
+
     # End to end through the public API, the call a user makes: a PanelMatrix
     # whose panels sit in page-locked host memory, and cholqr2 on it. Each
     # step uploads the panels, runs the device-resident chain, writes Q back
@@ -535,7 +600,7 @@ def run_ours(args):
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
                      "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
-        "tensor_form": tensor_form,
+        "tensor_form": tensor_form, "batched": batched,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

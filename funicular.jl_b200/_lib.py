@@ -108,6 +108,13 @@ SIGNATURES = {
     "fb_zgram_tc_workspace_size": [_i64, _int, _psz],
     "fb_zgram_tc": [_vp, _i64, _vp, _i64, _i64, _int, Z128, Z128, _vp, _sz, _vp],
     "fb_zlaplace7_apply": [_vp, _i64, _vp, _i64, _int, _int, _int, _int, Z128, _vp],
+    "fb_graph_capture_begin": [_vp],
+    "fb_graph_capture_end": [_vp, _pvp],
+    "fb_graph_launch": [_vp, _vp],
+    "fb_graph_destroy": [_vp],
+    "fb_zcholqr2_batched_workspace_size": [_vp, _vp, _int, _psz],
+    "fb_zcholqr2_batched": [_vp, _vp, _vp, _vp, _vp, _vp, _int, _int, _vp, _sz, _vp],
+    "fb_zcholqr2_batched_query": [_vp, _int, _vp, _vp],
     "fb_ghost_fill": [_vp, _int, _i64, _i64, _i64, _i64, _i64, ctypes.c_uint64, _int, _vp],
 }
 _RESTYPES = {"fb_last_error": ctypes.c_char_p, "fb_abi_version": ctypes.c_int,

@@ -81,8 +81,11 @@ int fb_zcholqr2_workspace_size(int64_t N, int k, size_t* bytes) {
     return FB_OK;
 }
 
+// The chain of one instance. status, when given, replaces the workspace's own
+// status block (a batch keeps one status per instance and shares the rest).
 static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info,
-                         int* passes, void* workspace, size_t workspace_bytes, fb_queue_t queue, bool tensor) {
+                         int* passes, void* workspace, size_t workspace_bytes, fb_queue_t queue, bool tensor,
+                         ChainStatus* status = nullptr) {
     if (N < 1 || k < 1) {
         set_error(FB_EINVAL, "cholqr2!: N and k must be positive, got N=%lld, k=%d", (long long)N, k);
         return FB_EINVAL;
@@ -100,7 +103,7 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
         return FB_ENOMEM;
     }
     char* ws = static_cast<char*>(workspace);
-    ChainStatus* st = reinterpret_cast<ChainStatus*>(ws + L.status);
+    ChainStatus* st = status ? status : reinterpret_cast<ChainStatus*>(ws + L.status);
     z64* G = reinterpret_cast<z64*>(ws + L.G);
     z64* U = reinterpret_cast<z64*>(ws + L.U);
     z64* Ra = reinterpret_cast<z64*>(ws + L.Ra);
@@ -134,10 +137,15 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
 
     if (info) {
         FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-        return fb_zcholqr2_query(workspace, info, passes, nullptr);
+        return fb_zcholqr2_query(st, info, passes, nullptr);
     }
     return FB_OK;
 }
+
+// A batch: one status block per instance, then one scratch area sized for
+// the largest instance, reused by every instance in turn (they run one after
+// another on the queue).
+static size_t batch_status_bytes(int count) { return align_up((size_t)count * sizeof(ChainStatus), 256); }
 
 int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
                 void* workspace, size_t workspace_bytes, fb_queue_t queue) {
@@ -151,6 +159,72 @@ int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_
         return FB_ENOTSUP;
     }
     return cholqr2_chain(Y, ldy, N, k, R, ldr, info, passes, workspace, workspace_bytes, queue, true);
+}
+
+int fb_zcholqr2_batched_workspace_size(const int64_t* N, const int* k, int count, size_t* bytes) {
+    if (!bytes || count < 0 || (count > 0 && (!N || !k))) {
+        set_error(FB_EINVAL, "fb_zcholqr2_batched_workspace_size: bad argument");
+        return FB_EINVAL;
+    }
+    size_t scratch = 0;
+    for (int i = 0; i < count; ++i) {
+        if (N[i] < 1 || k[i] < 1) {
+            set_error(FB_EINVAL, "cholqr2! batch: instance %d has N=%lld, k=%d", i, (long long)N[i], k[i]);
+            return FB_EINVAL;
+        }
+        const size_t t = cholqr_layout(N[i], k[i]).total;
+        if (t > scratch) scratch = t;
+    }
+    *bytes = batch_status_bytes(count) + scratch;
+    return FB_OK;
+}
+
+int fb_zcholqr2_batched(fb_z128* const* Y, const int64_t* ldy, const int64_t* N, const int* k, fb_z128* const* R,
+                        const int64_t* ldr, int count, int tensor_form, void* workspace, size_t workspace_bytes,
+                        fb_queue_t queue) {
+    if (count < 0 || (count > 0 && (!Y || !ldy || !N || !k || !R || !ldr))) {
+        set_error(FB_EINVAL, "fb_zcholqr2_batched: NULL argument array");
+        return FB_EINVAL;
+    }
+    if (count == 0) return FB_OK;
+    size_t need = 0;
+    FB_TRY(fb_zcholqr2_batched_workspace_size(N, k, count, &need));
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255)) {
+        set_error(FB_ENOMEM, "fb_zcholqr2_batched: workspace must be 256-byte aligned and hold %zu bytes (got %zu)",
+                  need, workspace_bytes);
+        return FB_ENOMEM;
+    }
+    ChainStatus* status = static_cast<ChainStatus*>(workspace);
+    char* scratch = static_cast<char*>(workspace) + batch_status_bytes(count);
+    const size_t scratch_bytes = workspace_bytes - batch_status_bytes(count);
+    for (int i = 0; i < count; ++i) {
+        if (tensor_form && k[i] > 64) {
+            set_error(FB_ENOTSUP, "cholqr2! batch: the tensor-core form handles k <= 64, instance %d has k=%d", i, k[i]);
+            return FB_ENOTSUP;
+        }
+        FB_TRY(cholqr2_chain(Y[i], ldy[i], N[i], k[i], R[i], ldr[i], nullptr, nullptr, scratch, scratch_bytes, queue,
+                             tensor_form != 0, status + i));
+    }
+    return FB_OK;
+}
+
+int fb_zcholqr2_batched_query(const void* workspace, int count, int* info, int* passes) {
+    if (!workspace || count < 0) { set_error(FB_EINVAL, "fb_zcholqr2_batched_query: bad argument"); return FB_EINVAL; }
+    int first_failed = -1;
+    for (int i = 0; i < count; ++i) {
+        int inf = 0, pas = 0;
+        const int st = fb_zcholqr2_query(static_cast<const ChainStatus*>(workspace) + i, &inf, &pas, nullptr);
+        if (st != FB_OK && st != FB_ENOTSPD) return st;
+        if (info) info[i] = inf;
+        if (passes) passes[i] = pas;
+        if (inf && first_failed < 0) first_failed = i;
+    }
+    if (first_failed >= 0) {
+        set_error(FB_ENOTSPD, "cholqr2! batch: the Gram matrix of instance %d is not positive definite even after "
+                  "the shift", first_failed);
+        return FB_ENOTSPD;
+    }
+    return FB_OK;
 }
 
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shifts) {

@@ -241,6 +241,36 @@ int fb_sync_all(void) {
     return FB_OK;
 }
 
+int fb_graph_capture_begin(fb_queue_t queue) {
+    if (!queue) { set_error(FB_EINVAL, "fb_graph_capture_begin: the default stream cannot be captured"); return FB_EINVAL; }
+    FB_CUDA(cudaStreamBeginCapture(static_cast<cudaStream_t>(queue), cudaStreamCaptureModeThreadLocal),
+            "cudaStreamBeginCapture");
+    return FB_OK;
+}
+
+int fb_graph_capture_end(fb_queue_t queue, fb_graph_t* graph) {
+    if (!queue || !graph) { set_error(FB_EINVAL, "fb_graph_capture_end: NULL argument"); return FB_EINVAL; }
+    cudaGraph_t g = nullptr;
+    FB_CUDA(cudaStreamEndCapture(static_cast<cudaStream_t>(queue), &g), "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t err = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    FB_CUDA(err, "cudaGraphInstantiate");
+    *graph = exec;
+    return FB_OK;
+}
+
+int fb_graph_launch(fb_graph_t graph, fb_queue_t queue) {
+    if (!graph) { set_error(FB_EINVAL, "fb_graph_launch: NULL graph"); return FB_EINVAL; }
+    FB_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(graph), static_cast<cudaStream_t>(queue)), "cudaGraphLaunch");
+    return FB_OK;
+}
+
+int fb_graph_destroy(fb_graph_t graph) {
+    if (graph) FB_CUDA(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph)), "cudaGraphExecDestroy");
+    return FB_OK;
+}
+
 int fb_copy2d(void* dst, size_t dpitch, const void* src, size_t spitch,
               size_t width_bytes, size_t cols, fb_queue_t queue) {
     if (width_bytes == 0 || cols == 0) return FB_OK;

@@ -191,6 +191,25 @@ def _destroy_event(h):
         pass
 
 
+class Graph:
+    """A captured sequence of the library's launches (fb_graph_capture_end),
+    replayed with one launch."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        self._finalizer = weakref.finalize(self, _destroy_graph, handle)
+
+    def launch(self, queue) -> None:
+        call("fb_graph_launch", ctypes.c_void_p(self.handle), ctypes.c_void_p(queue.handle if queue else None))
+
+
+def _destroy_graph(h):
+    try:
+        load().fb_graph_destroy(ctypes.c_void_p(h))
+    except Exception:
+        pass
+
+
 class HostSlab:
     """alloc_host_slab's result (src/device_api.jl:144-163): page-locked host
     memory, 64-byte aligned, handing out Fortran-ordered matrix views."""
@@ -340,6 +359,22 @@ class B200Backend:
             copy_region(dst, staging, q)
         self.sync_queue(q)
         return self.record_event(q) if queue is not None else None
+
+    def capture(self, queue, work) -> Graph:
+        """Runs work() with every launch on `queue` captured instead of run, and
+        returns the graph that replays them. Scratch used inside must not move
+        afterwards: pass kernels their own workspace."""
+        call("fb_graph_capture_begin", ctypes.c_void_p(queue.handle))
+        previous = self.current_queue
+        self._local.queue = queue
+        handle = ctypes.c_void_p()
+        try:
+            work()
+        finally:
+            self._local.queue = previous
+            status = load().fb_graph_capture_end(ctypes.c_void_p(queue.handle), ctypes.byref(handle))
+        check(status, "fb_graph_capture_end")
+        return Graph(handle.value)
 
     # -- helpers -----------------------------------------------------------
     def todevice(self, a: np.ndarray) -> DeviceMatrix:

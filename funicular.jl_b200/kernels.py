@@ -223,3 +223,68 @@ def laplace7_apply(backend, dst: DeviceMatrix, src: DeviceMatrix, grid, shift) -
     call("fb_zlaplace7_apply", _vp(dst.ptr), ctypes.c_int64(dst.ld), _vp(src.ptr), ctypes.c_int64(src.ld),
          nx, ny, nz, dst.cols, z128(shift), backend.queue_handle())
     return dst
+
+
+def cholqr2_batched_workspace_bytes(shapes) -> int:
+    """Device scratch for a batch of cholqr2! instances of the given (N, k)."""
+    n = len(shapes)
+    Ns = (ctypes.c_int64 * max(n, 1))(*[int(s[0]) for s in shapes])
+    ks = (ctypes.c_int * max(n, 1))(*[int(s[1]) for s in shapes])
+    need = ctypes.c_size_t(0)
+    call("fb_zcholqr2_batched_workspace_size", ctypes.cast(Ns, ctypes.c_void_p), ctypes.cast(ks, ctypes.c_void_p),
+         n, ctypes.byref(need))
+    return need.value
+
+
+def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, workspace=None):
+    """cholqr2! of many independent device matrices Ys[i] (N_i x k_i), R_i into
+    Rs[i], enqueued one after another on the current queue. With wait=True it
+    returns the list of passes and raises NotPositiveDefinite if an instance's
+    Gram stayed indefinite. `workspace` = (pointer, bytes) of caller-owned
+    scratch, which a captured graph needs (the backend's shared scratch may
+    move); by default the backend's is used."""
+    if form not in ("fp64", "tc"):
+        raise ArgumentError(f"cholqr2! form is 'fp64' or 'tc', got {form!r}")
+    if len(Ys) != len(Rs):
+        raise DimensionMismatch(f"a batch needs one R per Y, got {len(Ys)} and {len(Rs)}")
+    n = len(Ys)
+    for Y, R in zip(Ys, Rs):
+        _need_complex128(Y, R)
+        if R.shape != (Y.cols, Y.cols):
+            raise DimensionMismatch(f"cholqr2! of an {Y.shape} matrix writes a {Y.cols}x{Y.cols} R, got {R.shape}")
+    if n == 0:
+        return []
+    arr = lambda ctype, vals: (ctype * n)(*vals)
+    Yp = arr(ctypes.c_void_p, [Y.ptr for Y in Ys])
+    ldy = arr(ctypes.c_int64, [Y.ld for Y in Ys])
+    Ns = arr(ctypes.c_int64, [Y.rows for Y in Ys])
+    ks = arr(ctypes.c_int, [Y.cols for Y in Ys])
+    Rp = arr(ctypes.c_void_p, [R.ptr for R in Rs])
+    ldr = arr(ctypes.c_int64, [R.ld for R in Rs])
+    cast = lambda a: ctypes.cast(a, ctypes.c_void_p)
+    own = workspace is None
+    if own:
+        ws, ws_bytes = backend.workspace(cholqr2_batched_workspace_bytes([Y.shape for Y in Ys]))
+    else:
+        ws, ws_bytes = workspace
+    lib = _lib.load()
+    try:
+        status = lib.fb_zcholqr2_batched(cast(Yp), cast(ldy), cast(Ns), cast(ks), cast(Rp), cast(ldr), n,
+                                         1 if form == "tc" else 0, _vp(ws), ws_bytes, backend.queue_handle())
+    finally:
+        if own:
+            backend.workspace_release()
+    _lib.check(status, "cholqr2! batch")
+    if not wait:
+        return None
+    if backend.current_queue is not None:
+        backend.sync_queue(backend.current_queue)
+    else:
+        backend.sync_all()
+    info = (ctypes.c_int * n)()
+    passes = (ctypes.c_int * n)()
+    status = lib.fb_zcholqr2_batched_query(_vp(ws), n, cast(info), cast(passes))
+    if status == _lib.FB_ENOTSPD:
+        raise NotPositiveDefinite(_lib.last_error())
+    _lib.check(status, "cholqr2! batch")
+    return list(passes)

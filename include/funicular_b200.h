@@ -51,6 +51,7 @@ enum fb_eltype { FB_C128 = 0, FB_C64 = 1, FB_F64 = 2, FB_F32 = 3 };
 typedef struct { double re, im; } fb_z128;
 typedef void* fb_queue_t;
 typedef void* fb_event_t;
+typedef void* fb_graph_t;
 
 /* ---- library ---------------------------------------------------------- */
 
@@ -100,6 +101,17 @@ int fb_event_sync(fb_event_t event);
 /* *done = 1 once the event has been signalled. */
 int fb_event_query(fb_event_t event, int* done);
 int fb_sync_all(void);
+
+/* Stream capture into a CUDA graph, for callers that replay a fixed
+ * sequence of launches (a batch of cholqr2! instances, a whole sweep step).
+ * No counterpart in the reference's device API. Capture begins on a queue
+ * (not NULL), every library call that enqueues on that queue until
+ * fb_graph_capture_end is recorded instead of run, and the instantiated graph
+ * replays them with one fb_graph_launch. Pointers and sizes are baked in. */
+int fb_graph_capture_begin(fb_queue_t queue);
+int fb_graph_capture_end(fb_queue_t queue, fb_graph_t* graph);
+int fb_graph_launch(fb_graph_t graph, fb_queue_t queue);
+int fb_graph_destroy(fb_graph_t graph);
 
 /* h2d!/d2h! and device-to-device copies (src/device_api.jl:37,45;
  * copy_region! at ext/FunicularCUDAExt.jl:138-152): a 2-D copy of `cols`
@@ -243,6 +255,23 @@ int fb_zgram_tc(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda,
 int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k,
                    fb_z128* R, int64_t ldr, int* info, int* passes,
                    void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* Many independent cholqr2! instances of uneven N and k (the batched range
+ * finder; no counterpart in the reference, which orthonormalizes one
+ * PanelMatrix per call): instance i is Y[i] (N[i] x k[i], leading dimension
+ * ldy[i]) with its R in R[i] (ldr[i]). The instances' chains are enqueued one
+ * after another on `queue` and share one scratch area; each keeps its own
+ * status block, read by fb_zcholqr2_batched_query after the queue drained
+ * (info[i] = the failing pass or 0, passes[i] = 2 or 3). tensor_form != 0
+ * runs every Gram on the integer tensor cores (all k[i] <= 64). Nothing
+ * synchronizes, so the whole batch can be captured into one CUDA graph
+ * (fb_graph_capture_begin) and replayed with one launch. workspace:
+ * fb_zcholqr2_batched_workspace_size bytes, 256-byte aligned. */
+int fb_zcholqr2_batched_workspace_size(const int64_t* N, const int* k, int count, size_t* bytes);
+int fb_zcholqr2_batched(fb_z128* const* Y, const int64_t* ldy, const int64_t* N, const int* k,
+                        fb_z128* const* R, const int64_t* ldr, int count, int tensor_form,
+                        void* workspace, size_t workspace_bytes, fb_queue_t queue);
+int fb_zcholqr2_batched_query(const void* workspace, int count, int* info, int* passes);
 
 /* ---- ghost panels: src/ghosts.jl ------------------------------------- */
 

@@ -57,6 +57,8 @@ def parse_args():
     p.add_argument("--skip-cpu-baseline", action="store_true")
     p.add_argument("--batch", type=int, default=256,
                    help="instances of the batched cholqr2! measurement (0 skips it)")
+    p.add_argument("--adjoint-N", type=int, default=1 << 22,
+                   help="rows of the differentiation workload (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace"), default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
@@ -275,6 +277,108 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
             "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
             "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,
             "launch": "one fb_zcholqr2_batched call, replayed as one captured CUDA graph"}
+
+
+def run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier):
+    """The differentiation workload: N = args.adjoint_N (2^22), k = 64, the
+    loss real(tr(W^H Q)) + ||S||_F^2 with (Q, R) = cholqr2!(Y) and
+    S = Q^H (G Q), G Hermitian with 64 superdiagonals. Y, W and the band are
+    seeded device ghost fills (complex Gaussians), the band scaled by
+    sqrt(N / (129 k)) so that both terms of the loss are of the same order.
+    One step is the forward pass and the pullbacks the rrules run, on
+    preallocated buffers: copy Y, cholqr2!, G Q, 2 Q^H (G Q) (Sbar), W^H Q,
+    copy W into Qbar, the project pullback accumulated into Qbar, the cholqr2!
+    pullback written over Qbar. The gradient is checked against central
+    differences in 4 random directions (the tests use 32)."""
+    N, k, kd = args.adjoint_N, 64, 64
+    ghost = lambda dst, seed: fb.kernels.ghost_fill(backend, dst, 0, 0, seed, np.complex128)
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    alloc = lambda r, c: backend.alloc_device(np.complex128, (r, c))
+    YD = alloc(N, 2 * k)
+    Y, D = YD.view(slice(None), slice(0, k)), YD.view(slice(None), slice(k, 2 * k))
+    W, Q, GQ, Qbar = alloc(N, k), alloc(N, k), alloc(N, k), alloc(N, k)
+    R, Sbar, T = alloc(k, k), alloc(k, k), alloc(k, k)
+    ghost(Y, 0xC5)
+    ghost(W, 0xC6)
+    G = fb.HermitianBand.ghost(backend, N, kd, seed=0xC7, scale=float(np.sqrt(N / ((2 * kd + 1) * k))))
+    copy = fb.device_api.copy_region
+    K = fb.kernels
+
+    def forward(src):
+        copy(Q, src, queue)
+        K.cholqr2_resident(backend, Q, R, wait=False)
+        G.apply(backend, GQ, Q)
+        K.gram_accumulate(backend, Sbar, Q, GQ, 2.0, 0.0)
+        K.gram_accumulate(backend, T, W, Q, 1.0, 0.0)
+
+    def backward():
+        copy(Qbar, W, queue)
+        K.project_adjoint(backend, Qbar, GQ, Sbar, None, accumulate=True)
+        K.cholqr2_adjoint(backend, Qbar, Y, R, Qbar, None)
+
+    def loss():
+        backend.sync_queue(queue)
+        return float(np.real(np.trace(T.to_host())) + np.linalg.norm(Sbar.to_host() / 2) ** 2)
+
+    def timed(fn, reps):
+        for _ in range(max(1, args.warmup)):
+            backend.submit(queue, fn)
+        backend.sync_queue(queue)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            backend.submit(queue, fn)
+        b.record(stream)
+        b.synchronize()
+        return max_over_ranks(a.elapsed_time(b) / reps)
+
+    reps = max(3, min(args.steps, 10))
+    ms_step = timed(lambda: (forward(Y), backward()), reps)
+    ms_forward = timed(lambda: forward(Y), reps)
+    ms_cholqr2_pullback = timed(lambda: K.cholqr2_adjoint(backend, GQ, Y, R, Qbar, None), reps)
+    ms_project_pullback = timed(lambda: K.project_adjoint(backend, Qbar, GQ, Sbar, None, accumulate=True), reps)
+    ms_band = timed(lambda: G.apply(backend, GQ, Q), reps)
+    # The gradient, then central differences of the loss through the same
+    # forward kernels: Y +- h D is one product of [Y D] by [I; +-h I].
+    backend.submit(queue, lambda: (forward(Y), backward()))
+    loss0 = loss()
+    h = 1e-6
+    I = np.eye(k, dtype=np.complex128)
+    Cp, Cm = backend.todevice(np.vstack([I, h * I])), backend.todevice(np.vstack([I, -h * I]))
+    Yh = alloc(N, k)
+    fd, an = [], []
+    for i in range(4):
+        backend.submit(queue, lambda: ghost(D, 0x1000 + i))
+        vals = []
+        for C in (Cp, Cm):
+            backend.submit(queue, lambda: (K.rightmul_gemm(backend, Yh, YD, C), forward(Yh)))
+            vals.append(loss())
+        fd.append((vals[0] - vals[1]) / (2 * h))
+        backend.submit(queue, lambda: K.gram_accumulate(backend, T, Qbar, D, 1.0, 0.0))
+        backend.sync_queue(queue)
+        an.append(float(np.real(np.trace(T.to_host()))))
+    fd, an = np.array(fd), np.array(an)
+    fd_err = float(np.linalg.norm(fd - an) / np.linalg.norm(an))
+    flops_cp = 20.0 * N * k * k           # Qbar^H Y, Qbar R^-H (triangular), Y (R^-1 H R^-H)
+    flops_pp = 8.0 * N * k * k            # (G Q)(Sbar + Sbar^H)
+    flops_band = 8.0 * N * k * (2 * kd + 1)
+    del YD, W, Q, GQ, Qbar, Yh, G
+    return {
+        "workload": f"rrule through cholqr2! and project, N={N}, k={k}, G Hermitian band kd={kd}",
+        "ms_per_step": ms_step, "ms_forward": ms_forward, "loss": loss0,
+        "fd_rel_error": fd_err, "fd_directions": 4, "fd_step": h, "bound_fd": 1e-6,
+        "cholqr2_pullback": {"ms": ms_cholqr2_pullback, "tflops": flops_cp / (ms_cholqr2_pullback * 1e-3) / 1e12,
+                             "gbs": 80.0 * N * k / (ms_cholqr2_pullback * 1e-3) / 1e9,
+                             "per_launch": "20 N k^2 flops, 80 N k bytes (Qbar, Y read twice, Ybar written)"},
+        "project_pullback": {"ms": ms_project_pullback, "tflops": flops_pp / (ms_project_pullback * 1e-3) / 1e12,
+                             "gbs": 48.0 * N * k / (ms_project_pullback * 1e-3) / 1e9,
+                             "per_launch": "8 N k^2 flops, 48 N k bytes (G Q read, Qbar read and written)"},
+        "band_apply": {"ms": ms_band, "tflops": flops_band / (ms_band * 1e-3) / 1e12,
+                       "per_launch": "8 N k (2 kd + 1) flops"},
+    }
 
 
 def reduce_max_over_ranks(x: float, world: int, device) -> float:
@@ -544,6 +648,14 @@ def run_ours(args):
     batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.batch > 0 else None)
 
+    adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
+               if args.adjoint_N > 0 else None)
+    if adjoint is not None:
+        fp = adjoint["cholqr2_pullback"]["tflops"]
+        adjoint["cholqr2_pullback"]["fp64_frac"] = fp / fp64_peak
+        adjoint["project_pullback"]["fp64_frac"] = adjoint["project_pullback"]["tflops"] / fp64_peak
+        adjoint["band_apply"]["fp64_frac"] = adjoint["band_apply"]["tflops"] / fp64_peak
+
     # End to end through the public API, the call a user makes: a PanelMatrix
     # whose panels sit in page-locked host memory, and cholqr2 on it. Each
     # step uploads the panels, runs the device-resident chain, writes Q back
@@ -600,7 +712,7 @@ def run_ours(args):
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
                      "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
-        "tensor_form": tensor_form, "batched": batched,
+        "tensor_form": tensor_form, "batched": batched, "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

@@ -19,8 +19,10 @@ from .panels import PanelMatrix, free
 from .executor import (sweep, foreachpanel, readpanels, writepanels, updatepanels, PanelSteps, RowSteps,
                        rowtraversal)
 from .panelblas import (gram, panelmul, cholqr2, project, rightmul, DenseOperator, ColumnOperator,
-                        DeviceOperator, Laplacian7, cholesky_upper)
+                        DeviceOperator, Laplacian7, HermitianBand, cholesky_upper)
 from .ghosts import GhostPanels, isghost
+from . import autodiff
+from .autodiff import rrule
 
 __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceError",
            "OutOfDeviceMemory", "B200Backend", "DeviceMatrix", "HostSlab", "b200_backend",
@@ -28,4 +30,5 @@ __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceE
            "device_bytes_allocated", "host_bytes_reserved", "host_bytes_in_use", "host_bytes_free",
            "PanelMatrix", "free", "sweep", "foreachpanel", "readpanels", "writepanels", "updatepanels",
            "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "project", "rightmul",
-           "DenseOperator", "ColumnOperator", "DeviceOperator", "Laplacian7", "cholesky_upper", "GhostPanels", "isghost"]
+           "DenseOperator", "ColumnOperator", "DeviceOperator", "Laplacian7", "HermitianBand", "cholesky_upper", "GhostPanels", "isghost",
+           "autodiff", "rrule"]

@@ -288,3 +288,74 @@ def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, work
         raise NotPositiveDefinite(_lib.last_error())
     _lib.check(status, "cholqr2! batch")
     return list(passes)
+
+
+# ---- differentiation: the pullbacks of cholqr2! and project ---------------------
+
+def cholqr2_adjoint(backend, Ybar: DeviceMatrix, Y: DeviceMatrix, R: DeviceMatrix,
+                    Qbar: DeviceMatrix | None = None, Rbar: DeviceMatrix | None = None) -> DeviceMatrix:
+    """The pullback of (Q, R) = cholqr2!(Y): Ybar <- (Qbar + Q H) R^-H with
+    H = copyltu(R Rbar^H - Qbar^H Q), Q recomputed from the original Y and R
+    inside the products. Qbar or Rbar None is a zero cotangent; Ybar may be
+    Qbar itself."""
+    _need_complex128(Ybar, Y, R, *(m for m in (Qbar, Rbar) if m is not None))
+    N, k = Y.shape
+    if Ybar.shape != (N, k) or R.shape != (k, k):
+        raise DimensionMismatch(f"the cholqr2! pullback of an {N}x{k} Y takes a {k}x{k} R and writes an {N}x{k} "
+                                f"Ybar, got R {R.shape} and Ybar {Ybar.shape}")
+    if Qbar is not None and Qbar.shape != (N, k):
+        raise DimensionMismatch(f"Qbar must be {N}x{k}, got {Qbar.shape}")
+    if Rbar is not None and Rbar.shape != (k, k):
+        raise DimensionMismatch(f"Rbar must be {k}x{k}, got {Rbar.shape}")
+    if Ybar.size == 0:
+        return Ybar
+    need = ctypes.c_size_t(0)
+    call("fb_zcholqr2_adjoint_workspace_size", ctypes.c_int64(N), k, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    try:
+        call("fb_zcholqr2_adjoint", _vp(Ybar.ptr), Ybar.ld, _vp(Y.ptr), Y.ld, _vp(R.ptr), R.ld,
+             _vp(Qbar.ptr if Qbar is not None else None), Qbar.ld if Qbar is not None else 0,
+             _vp(Rbar.ptr if Rbar is not None else None), Rbar.ld if Rbar is not None else 0,
+             ctypes.c_int64(N), k, _vp(ws), ws_bytes, backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    return Ybar
+
+
+def project_adjoint(backend, Qbar: DeviceMatrix, GQ: DeviceMatrix, Sbar: DeviceMatrix,
+                    GhQ: DeviceMatrix | None = None, accumulate: bool = False) -> DeviceMatrix:
+    """The pullback of S = project(Q, G) = Q^H (G Q) with respect to Q:
+    Qbar <- [Qbar +] (G Q) Sbar^H + (G^H Q) Sbar, from the operator images
+    GQ and GhQ; GhQ None means G is Hermitian."""
+    _need_complex128(Qbar, GQ, Sbar, *(m for m in (GhQ,) if m is not None))
+    N, k = GQ.shape
+    if Qbar.shape != (N, k) or Sbar.shape != (k, k) or (GhQ is not None and GhQ.shape != (N, k)):
+        raise DimensionMismatch(f"the project pullback maps a {k}x{k} Sbar and {N}x{k} images to an {N}x{k} Qbar, "
+                                f"got Sbar {Sbar.shape}, Qbar {Qbar.shape}")
+    if Qbar.size == 0:
+        return Qbar
+    need = ctypes.c_size_t(0)
+    call("fb_zproject_adjoint_workspace_size", k, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    try:
+        call("fb_zproject_adjoint", _vp(Qbar.ptr), Qbar.ld, _vp(GQ.ptr), GQ.ld,
+             _vp(GhQ.ptr if GhQ is not None else None), GhQ.ld if GhQ is not None else 0,
+             _vp(Sbar.ptr), Sbar.ld, ctypes.c_int64(N), k, 1 if accumulate else 0, _vp(ws), ws_bytes,
+             backend.queue_handle())
+    finally:
+        backend.workspace_release()
+    return Qbar
+
+
+def hband_apply(backend, dst: DeviceMatrix, src: DeviceMatrix, Dg: DeviceMatrix) -> DeviceMatrix:
+    """dst <- G src for the Hermitian band G stored by diagonals in Dg
+    (N x (kd + 1), column d the d-th superdiagonal)."""
+    _need_complex128(dst, src, Dg)
+    N = Dg.rows
+    if src.rows != N or tuple(dst.shape) != tuple(src.shape):
+        raise DimensionMismatch(f"a {N}x{N} band operator maps {N}-row panels, got {src.shape} -> {dst.shape}")
+    if dst.size == 0:
+        return dst
+    call("fb_zhband_apply", _vp(dst.ptr), ctypes.c_int64(dst.ld), _vp(src.ptr), ctypes.c_int64(src.ld),
+         _vp(Dg.ptr), ctypes.c_int64(Dg.ld), ctypes.c_int64(N), Dg.cols - 1, dst.cols, backend.queue_handle())
+    return dst

@@ -69,9 +69,17 @@ class DeviceOperator:
 
     panel_capable = True
     shape = (0, 0)
+    # Whether G^H = G, which lets the pullback of project skip applying G^H.
+    hermitian = False
 
     def apply(self, backend, dst: DeviceMatrix, src: DeviceMatrix):
         raise NotImplementedError
+
+    def adjoint(self) -> "DeviceOperator":
+        """G^H, which the pullback of project applies when G is not Hermitian."""
+        if self.hermitian:
+            return self
+        raise ArgumentError(f"{type(self).__name__} has no adjoint; the pullback of project needs G^H")
 
 
 class DenseOperator(DeviceOperator):
@@ -80,11 +88,17 @@ class DenseOperator(DeviceOperator):
 
     def __init__(self, backend, G: np.ndarray):
         G = np.asfortranarray(np.asarray(G, dtype=np.complex128))
+        self.backend = backend
+        self.host = G
         self.G = backend.todevice(G)
         self.shape = G.shape
+        self.hermitian = G.shape[0] == G.shape[1] and bool(np.array_equal(G, G.conj().T))
 
     def apply(self, backend, dst, src):
         kernels.rightmul_gemm(backend, dst, self.G, src)
+
+    def adjoint(self):
+        return self if self.hermitian else DenseOperator(self.backend, self.host.conj().T)
 
 
 class Laplacian7(DeviceOperator):
@@ -103,6 +117,50 @@ class Laplacian7(DeviceOperator):
     def apply(self, backend, dst, src):
         kernels.laplace7_apply(backend, dst, src, self.grid, self.shift)
 
+    @property
+    def hermitian(self):
+        return self.shift.imag == 0
+
+    def adjoint(self):
+        return Laplacian7(self.grid, self.shift.conjugate())
+
+
+class HermitianBand(DeviceOperator):
+    """A Hermitian N x N operator with kd superdiagonals, held on the device
+    by diagonals: Dg is N x (kd + 1) with Dg[i, d] = G[i, i + d] (the imaginary
+    part of the main diagonal and the entries past the matrix are ignored).
+    The operator of the differentiation workload."""
+
+    hermitian = True
+
+    def __init__(self, backend, Dg):
+        if isinstance(Dg, DeviceMatrix):
+            self.Dg = Dg
+        else:
+            Dg = np.asfortranarray(np.asarray(Dg, dtype=np.complex128))
+            if Dg.ndim != 2 or Dg.shape[1] < 1:
+                raise ArgumentError(f"band storage is N x (kd + 1), got shape {Dg.shape}")
+            self.Dg = backend.todevice(Dg)
+        self.kd = self.Dg.cols - 1
+        self.shape = (self.Dg.rows, self.Dg.rows)
+
+    @classmethod
+    def ghost(cls, backend, N: int, kd: int, seed: int, scale: float = 1.0) -> "HermitianBand":
+        """The seeded band: entry (i, d) of the storage is scale times the
+        complex Gaussian of a ComplexF64 GhostPanels matrix (seed) at row i,
+        column d, filled on the device."""
+        Dg = backend.alloc_device(np.complex128, (N, kd + 1))
+        kernels.ghost_fill(backend, Dg, 0, 0, seed, np.complex128)
+        if scale != 1.0:
+            S = backend.todevice(np.eye(kd + 1, dtype=np.complex128) * scale)
+            out = backend.alloc_device(np.complex128, (N, kd + 1))
+            kernels.rightmul_gemm(backend, out, Dg, S)
+            Dg = out
+        return cls(backend, Dg)
+
+    def apply(self, backend, dst, src):
+        kernels.hband_apply(backend, dst, src, self.Dg)
+
 
 class ColumnOperator(DeviceOperator):
     """Wraps an operator so it is applied column by column (the reference's
@@ -116,6 +174,13 @@ class ColumnOperator(DeviceOperator):
 
     def apply(self, backend, dst, src):
         self.inner.apply(backend, dst, src)
+
+    @property
+    def hermitian(self):
+        return self.inner.hermitian
+
+    def adjoint(self):
+        return self if self.hermitian else ColumnOperator(self.inner.adjoint())
 
 
 def apply_operator(backend, Y: DeviceMatrix, G: DeviceOperator, X: DeviceMatrix):

@@ -273,6 +273,52 @@ int fb_zcholqr2_batched(fb_z128* const* Y, const int64_t* ldy, const int64_t* N,
                         void* workspace, size_t workspace_bytes, fb_queue_t queue);
 int fb_zcholqr2_batched_query(const void* workspace, int count, int* info, int* passes);
 
+/* ---- differentiation: the adjoints behind the rrules ------------------
+ * The reference has no rrule (Project.toml:6-9 has no ChainRulesCore); these
+ * are the kernels a ChainRulesCore.rrule for cholqr2! (src/panelblas.jl:130)
+ * and project (src/panelblas.jl:268) calls in its pullback. */
+
+/* The pullback of (Q, R) = cholqr2!(Y): Ybar <- (Qbar + Q H) R^-H with
+ * H = copyltu(R Rbar^H - Qbar^H Q) (the Hermitian matrix with the strictly
+ * lower triangle of its argument, that triangle's conjugate transpose above
+ * the diagonal and the real part of the diagonal on it). Y is the ORIGINAL
+ * input (N x k) and R the factor cholqr2! returned: Q is recomputed as
+ * Y R^-1 inside the products, never stored. Qbar (N x k) and Rbar (k x k) may
+ * each be NULL for a zero cotangent; only Rbar's upper triangle and the real
+ * part of its diagonal matter. Ybar may be Qbar itself (same pointer and
+ * leading dimension) and must not overlap Y. Runs on the FP64 tensor cores
+ * for k <= 64 (DMMA), on the FP64 pipes past that. workspace:
+ * fb_zcholqr2_adjoint_workspace_size bytes, 256-byte aligned. Enqueues only. */
+int fb_zcholqr2_adjoint_workspace_size(int64_t N, int k, size_t* bytes);
+int fb_zcholqr2_adjoint(fb_z128* Ybar, int64_t ldyb, const fb_z128* Y, int64_t ldy,
+                        const fb_z128* R, int64_t ldr, const fb_z128* Qbar, int64_t ldqb,
+                        const fb_z128* Rbar, int64_t ldrb, int64_t N, int k,
+                        void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* The pullback of S = project(Q, G) = Q^H (G Q) with respect to Q:
+ * Qbar <- [Qbar +] (G Q) Sbar^H + (G^H Q) Sbar, with GQ = G Q and GhQ =
+ * G^H Q the operator images the caller computed (N x k). GhQ == NULL means G
+ * is Hermitian: then Qbar gets (G Q)(Sbar + Sbar^H) in one product.
+ * accumulate != 0 adds to Qbar, 0 overwrites it (NaN in it included). Qbar
+ * must not overlap GQ or GhQ. workspace: fb_zproject_adjoint_workspace_size
+ * bytes, 256-byte aligned. Enqueues only. */
+int fb_zproject_adjoint_workspace_size(int k, size_t* bytes);
+int fb_zproject_adjoint(fb_z128* Qbar, int64_t ldqb, const fb_z128* GQ, int64_t ldgq,
+                        const fb_z128* GhQ, int64_t ldghq, const fb_z128* Sbar, int64_t ldsb,
+                        int64_t N, int k, int accumulate,
+                        void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* A Hermitian band operator (the G of the differentiation workload; no
+ * counterpart in the reference, whose operators are user callables behind
+ * apply_operator!, src/operator.jl:80-87): Y[:, c] <- G X[:, c] for c < cols,
+ * G N x N Hermitian with kd superdiagonals, stored by diagonals: Dg is
+ * N x (kd + 1), leading dimension lddg, Dg[i + d lddg] = G[i, i + d]
+ * (entries with i + d >= N are ignored, as is the imaginary part of the main
+ * diagonal). Y and X must not overlap. */
+int fb_zhband_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx,
+                    const fb_z128* Dg, int64_t lddg, int64_t N, int kd, int cols,
+                    fb_queue_t queue);
+
 /* ---- ghost panels: src/ghosts.jl ------------------------------------- */
 
 /* The device fill behind GhostPanels(T, N, k; seed) (replaces the host

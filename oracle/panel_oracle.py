@@ -273,3 +273,77 @@ def laplacian7(grid, shift):
     L = (sp.kron(I(nz), sp.kron(I(ny), d2(nx))) + sp.kron(I(nz), sp.kron(d2(ny), I(nx)))
          + sp.kron(d2(nz), sp.kron(I(ny), I(nx))))
     return (L + shift * I(nx * ny * nz)).tocsr().astype(np.complex128)
+
+
+# ---- differentiation: the pullbacks behind the rrules --------------------------
+# The reference has no rrule (Project.toml:6-9 has no ChainRulesCore), so
+# nothing in it pins these; they are the textbook reverse-mode rules of the
+# functions above, pinned in tests/test_adjoint_oracle.py by central finite
+# differences of cholqr2 and project as defined in this module.
+
+def copyltu(M):
+    """The Hermitian matrix with M's strictly lower triangle, its conjugate
+    transpose above the diagonal and Re diag(M) on the diagonal."""
+    L = np.tril(M, -1)
+    return L + L.conj().T + np.diag(np.diag(M).real)
+
+
+def cholqr2_adjoint(Y, R, Qbar=None, Rbar=None):
+    """The pullback of (Q, R) = cholqr2!(Y) (src/panelblas.jl:130-146), which
+    is the thin QR factorization with a positive real diagonal in R: for a
+    real loss, Ybar = (Qbar + Q H) R^-H with H = copyltu(R Rbar^H - Qbar^H Q).
+    Q is recomputed from Y and R (Q = Y R^-1), as the device kernel does."""
+    import scipy.linalg as sla
+    N, k = Y.shape
+    Q = sla.solve_triangular(R, Y.T, trans="T", lower=False).T  # Y R^-1
+    M = np.zeros((k, k), dtype=np.complex128)
+    if Rbar is not None:
+        M += R @ Rbar.conj().T
+    if Qbar is not None:
+        M -= Qbar.conj().T @ Q
+    Z = Q @ copyltu(M)
+    if Qbar is not None:
+        Z = Z + Qbar
+    # Z R^-H: solve X R^H = Z, i.e. R X^H = Z^H.
+    return sla.solve_triangular(R, Z.conj().T, lower=False).conj().T
+
+
+def project_adjoint(Q, G, Sbar):
+    """The pullback of S = project(Q, G) = Q^H (G Q) (src/panelblas.jl:268-301)
+    with respect to Q: Qbar = (G Q) Sbar^H + (G^H Q) Sbar."""
+    GhT = G.conj().T
+    return (G @ Q) @ Sbar.conj().T + (GhT @ Q) @ Sbar
+
+
+def hermitian_band(Dg):
+    """The sparse N x N Hermitian matrix stored by diagonals in Dg (N x
+    (kd + 1), Dg[i, d] = G[i, i + d]; the imaginary part of the main diagonal
+    and the entries past the matrix ignored)."""
+    import scipy.sparse as sp
+    N, kd1 = Dg.shape
+    diags, offs = [Dg[:, 0].real.astype(np.complex128)], [0]
+    for d in range(1, kd1):
+        if d >= N:
+            break
+        diags += [Dg[:N - d, d], Dg[:N - d, d].conj()]
+        offs += [d, -d]
+    return sp.diags(diags, offs, shape=(N, N), format="csr", dtype=np.complex128)
+
+
+def range_finder_loss(Y, W, G, w=None):
+    """The differentiation workload's loss: real(tr(W^H Q)) + ||S||_F^2 with
+    (Q, R) = cholqr2!(copy(Y)) and S = project(Q, G)."""
+    Q = np.array(Y, dtype=np.complex128, order="F", copy=True)
+    cholqr2(Q, w)
+    S = project(Q, G, w)
+    return float(np.real(np.vdot(W, Q)) + np.linalg.norm(S) ** 2)
+
+
+def range_finder_gradient(Y, W, G):
+    """Ybar of range_finder_loss: Qbar = W + (G Q)(2 S)^H + (G^H Q)(2 S), then
+    the cholqr2! pullback (Rbar = 0)."""
+    Q = np.array(Y, dtype=np.complex128, order="F", copy=True)
+    R, _ = cholqr2(Q)
+    S = project(Q, G)
+    Qbar = W + project_adjoint(Q, G, 2 * S)
+    return cholqr2_adjoint(Y, R, Qbar, None)

@@ -57,6 +57,8 @@ def parse_args():
     p.add_argument("--skip-cpu-baseline", action="store_true")
     p.add_argument("--batch", type=int, default=256,
                    help="instances of the batched cholqr2! measurement (0 skips it)")
+    p.add_argument("--wide-N", type=int, default=10_000_000,
+                   help="rows of the k = 128 configuration (0 skips it)")
     p.add_argument("--adjoint-N", type=int, default=1 << 22,
                    help="rows of the differentiation workload (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace"), default=None,
@@ -279,6 +281,50 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
             "launch": "one fb_zcholqr2_batched call, replayed as one captured CUDA graph"}
 
 
+def run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak):
+    """The wide configuration: plain FP64 cholqr2! at N = args.wide_N (10^7),
+    k = 128, on Y = U diag(s) V^H with condition numbers 1e4 and 1e7 (s
+    log-spaced). The triangular solves go by 64-column blocks. Each kappa: one
+    checked run (passes, ||Q^H Q - I||_F, ||Y - QR||/||Y||), then the timed
+    loop on the result, as in the main step."""
+    N, k = args.wide_N, 128
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    out = {"workload": f"cholqr2! FP64, N={N}, k={k}, ComplexF64 resident", "runs": []}
+    for kappa in (1e4, 1e7):
+        Yt0 = build_workload(fb, backend, torch, device, N, k, seed=0xC3 + int(np.log10(kappa)), kappa=kappa)
+        Yt = Yt0.clone()
+        torch.cuda.synchronize()
+        Y = wrap(fb, Yt, N, k)
+        R = backend.alloc_device(np.complex128, (k, k))
+        checked = {}
+        backend.submit(queue, lambda: checked.update(r=fb.kernels.cholqr2_resident(backend, Y, R)))
+        passes, _ = checked["r"]
+        orth, orth_cublas, recon = accuracy(fb, backend, torch, Yt0, Yt, R, N, k)
+        del Yt0
+        step = lambda: backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, R, wait=False))
+        for _ in range(args.warmup):
+            step()
+        backend.sync_queue(queue)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            step()
+        b.record(stream)
+        b.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b) / args.steps)
+        bound_ms = alg_flops(N, k) / (fp64_peak * 1e12) * 1e3
+        out["runs"].append({"kappa": kappa, "passes": passes, "ms_per_step": ms,
+                            "value": whole_job_gbs(alg_bytes(N, k), world, ms), "unit": UNIT,
+                            "tflops": alg_flops(N, k) / (ms * 1e-3) / 1e12, "fp64_roofline_frac": bound_ms / ms,
+                            "orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
+                            "reconstruction_rel": recon})
+        del Yt, Y
+    return out
+
+
 def run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier):
     """The differentiation workload: N = args.adjoint_N (2^22), k = 64, the
     loss real(tr(W^H Q)) + ||S||_F^2 with (Q, R) = cholqr2!(Y) and
@@ -427,9 +473,10 @@ def wrap(fb, tensor, rows, cols):
     return fb.DeviceMatrix(tensor.data_ptr(), (rows, cols), rows, _np.dtype(_np.complex128), tensor)
 
 
-def build_workload(fb, backend, torch, device, N, k, seed):
-    """Y = U diag(s) V^H on the device. U: a seeded complex Gaussian made
-    orthonormal by the backend's own cholqr2!; V: seeded Haar unitary."""
+def build_workload(fb, backend, torch, device, N, k, seed, kappa=1e6):
+    """Y = U diag(s) V^H on the device, s log-spaced from 1 to 1/kappa. U: a
+    seeded complex Gaussian made orthonormal by the backend's own cholqr2!;
+    V: seeded Haar unitary."""
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
     Ut = torch.randn((k, N), dtype=torch.complex128, device=device, generator=gen)
@@ -437,7 +484,7 @@ def build_workload(fb, backend, torch, device, N, k, seed):
     Rtmp = backend.alloc_device(np.complex128, (k, k))
     fb.kernels.cholqr2_resident(backend, U, Rtmp)
     V = haar_unitary(k, seed + 1)
-    s = 10.0 ** np.linspace(0, -6, k)
+    s = 10.0 ** np.linspace(0, -np.log10(kappa), k)
     C = backend.todevice(np.asfortranarray(s[:, None] * V.conj().T))
     Yt = torch.empty((k, N), dtype=torch.complex128, device=device)
     Y = wrap(fb, Yt, N, k)
@@ -648,6 +695,8 @@ def run_ours(args):
     batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.batch > 0 else None)
 
+    wide = (run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak)
+            if args.wide_N > 0 else None)
     adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.adjoint_N > 0 else None)
     if adjoint is not None:
@@ -712,7 +761,7 @@ def run_ours(args):
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
                      "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
-        "tensor_form": tensor_form, "batched": batched, "adjoint": adjoint,
+        "tensor_form": tensor_form, "batched": batched, "wide": wide, "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

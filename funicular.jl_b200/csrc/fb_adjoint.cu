@@ -20,16 +20,9 @@
 // (G Q)(Sbar + Sbar^H) when G is Hermitian. The caller applies the operator;
 // this file does the N x k by k x k products.
 //
-// The fused pass: D <- beta D + A1 L + A2 C, A1 and A2 N x k, L lower
-// triangular and C dense k x k, on the FP64 tensor cores (DMMA m8n8k4 on the
-// real form of the complex product, as the triangular solver does) for
-// k <= 64. A warp owns 8 rows at a time; it streams their entries one k-step
-// (two complex columns) at a time and keeps every output n-tile in its
-// accumulators, so each input entry is read once and each output written
-// once. L and C sit in shared memory as MMA B fragments ordered by k-step,
-// L keeping only the n-tiles on or below its diagonal.
-#include "fb_common.cuh"
-#include "fb_tma.cuh"
+// The fused pass is the tensor-core right product of fb_rmul.cuh with L = R^-H
+// (lower triangular) and C = R^-1 H R^-H.
+#include "fb_rmul.cuh"
 
 namespace fb {
 
@@ -39,52 +32,7 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
                  const ChainStatus* st, int gate);
 size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian);
 
-constexpr int AD_KMAX = 64;       // widest k of the tensor-core pass
-constexpr int AD_THREADS = 256;   // threads of the tensor-core pass
 constexpr int PREP_THREADS = 1024;
-
-// B fragments of one dense k x k factor: NT n-tiles x 2 NT k-steps x 32 lanes.
-__host__ __device__ inline int dense_frag_doubles(int nt) { return 64 * nt * nt; }
-// Of a lower triangular one: k-step s holds n-tiles 0 .. s/2.
-__host__ __device__ inline int lower_frag_doubles(int nt) { return 32 * nt * (nt + 1); }
-__host__ __device__ inline int lower_step_offset(int s) {
-    const int m = s >> 1;
-    return (s & 1) ? (m + 1) * (m + 1) : m * (m + 1);
-}
-
-// Entry (kr, nr) of the real 8 x 8 form of a complex 4 x 4 block M: kr = 2 i + p
-// (row i of M, part p of the input entry it multiplies), nr = 2 j + o (column
-// j, part o of the output).
-__device__ __forceinline__ double real_part_of(z64 m, int p, int o) {
-    return o == 0 ? (p == 0 ? m.x : -m.y) : (p == 0 ? m.y : m.x);
-}
-
-// The B fragment entry of `lane` for k-step s and n-tile t of a column-major
-// k x k matrix M (zero past k): lane & 3 is the real k index inside the
-// step, lane >> 2 the real n index inside the tile.
-__device__ __forceinline__ double frag_entry(const z64* M, int k, int s, int t, int lane) {
-    const int kr = lane & 3, nr = lane >> 2;
-    const int i = 2 * s + (kr >> 1), p = kr & 1;
-    const int j = 4 * t + (nr >> 1), o = nr & 1;
-    return (i < k && j < k) ? real_part_of(M[i + (int64_t)j * k], p, o) : 0.0;
-}
-
-__device__ void build_dense_frags(double* frag, const z64* M, int k, int nt) {
-    for (int e = threadIdx.x; e < dense_frag_doubles(nt); e += blockDim.x) {
-        const int lane = e & 31, q = e >> 5;
-        const int s = q / nt, t = q - s * nt;
-        frag[e] = frag_entry(M, k, s, t, lane);
-    }
-}
-
-__device__ void build_lower_frags(double* frag, const z64* M, int k, int nt) {
-    for (int e = threadIdx.x; e < lower_frag_doubles(nt); e += blockDim.x) {
-        const int lane = e & 31, q = e >> 5;
-        int s = 0;
-        while (lower_step_offset(s + 1) <= q) ++s;
-        frag[e] = frag_entry(M, k, s, q - lower_step_offset(s), lane);
-    }
-}
 
 __device__ __forceinline__ z64 zconj(z64 a) { return zmake(a.x, -a.y); }
 
@@ -149,10 +97,9 @@ cholqr2_adjoint_prep_kernel(const z64* __restrict__ R, int64_t ldr, const z64* _
         C[e] = c;
     }
     __syncthreads();
-    if (k <= AD_KMAX) {
-        const int nt = (k + 3) / 4;
-        build_dense_frags(fdense, C, k, nt);
-        build_lower_frags(flower, L, k, nt);
+    if (k <= RM_KMAX) {
+        build_dense_frags(fdense, C, k, k, k, 1.0);
+        build_lower_frags(flower, L, k, k);
     }
 }
 
@@ -170,170 +117,10 @@ project_adjoint_prep_kernel(const z64* __restrict__ Sbar, int64_t ldsb, int k, i
         C2[e] = s;
     }
     __syncthreads();
-    if (k <= AD_KMAX) {
-        const int nt = (k + 3) / 4;
-        build_dense_frags(f1, C1, k, nt);
-        if (!hermitian) build_dense_frags(f2, C2, k, nt);
+    if (k <= RM_KMAX) {
+        build_dense_frags(f1, C1, k, k, k, 1.0);
+        if (!hermitian) build_dense_frags(f2, C2, k, k, k, 1.0);
     }
-}
-
-// D <- beta D + A1 L + A2 C on the FP64 tensor cores (k <= 4 NT). A1 may be
-// NULL (no L term). D may be the same matrix as A1 or A2: a warp reads all of
-// its rows' inputs before it writes their outputs.
-template <int NT>
-__global__ void __launch_bounds__(AD_THREADS, 1)
-rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2, int64_t rows,
-                 int k, const double* __restrict__ gdense, const double* __restrict__ glower, z64 beta,
-                 int use_beta, int zero) {
-    constexpr int NS = 2 * NT;          // k-steps
-    constexpr int G = 4;                // k-steps whose inputs are loaded together
-    constexpr int NG = (NS + G - 1) / G;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* fd = reinterpret_cast<double*>(smem_raw);
-    double* fl = fd + dense_frag_doubles(NT);
-    const bool lower = A1 != nullptr;
-    {
-        const double2* s2 = reinterpret_cast<const double2*>(gdense);
-        double2* d2 = reinterpret_cast<double2*>(fd);
-        for (int e = threadIdx.x; e < dense_frag_doubles(NT) / 2; e += blockDim.x) d2[e] = s2[e];
-        if (lower) {
-            const double2* l2 = reinterpret_cast<const double2*>(glower);
-            double2* dl = reinterpret_cast<double2*>(fl);
-            for (int e = threadIdx.x; e < lower_frag_doubles(NT) / 2; e += blockDim.x) dl[e] = l2[e];
-        }
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rr = lane >> 2, cq = lane & 3, acol = cq >> 1, apart = lane & 1;
-    const int64_t units = (rows + 7) / 8;
-    const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; u < units; u += warps_total) {
-        const int64_t row = u * 8 + rr;
-        const bool live = row < rows;
-        const int64_t r0 = live ? row : 0;
-        // This lane's entries of k-steps gG .. gG + G - 1 of both inputs.
-        auto load_group = [&](int g, double (&b2)[G], double (&b1)[G], const z64* p2, const z64* p1) {
-#pragma unroll
-            for (int j = 0; j < G; ++j) {
-                const int s = g * G + j;
-                const int col = 2 * s + acol;
-                const bool ok = s < NS && live && col < k;
-                b2[j] = ok ? reinterpret_cast<const double*>(p2 + (int64_t)col * lda2)[apart] : 0.0;
-                b1[j] = (ok && lower) ? reinterpret_cast<const double*>(p1 + (int64_t)col * lda1)[apart] : 0.0;
-            }
-        };
-        double acc[NT][2];
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int col = 4 * t + cq;
-            z64 d = zmake(0.0, 0.0);
-            if (use_beta && live && col < k) d = zmul(beta, D[r0 + (int64_t)col * ldd]);
-            acc[t][0] = d.x;
-            acc[t][1] = d.y;
-        }
-        const z64* p2 = A2 + r0;
-        const z64* p1 = lower ? A1 + r0 : A2 + r0;
-        double c2[G], c1[G], n2[G], n1[G];
-        load_group(0, c2, c1, p2, p1);
-        load_group(1, n2, n1, p2, p1);
-        // Two groups of loads in flight: group g + 2 is issued once group
-        // g's products are done, so its registers are not held any longer.
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-#pragma unroll
-            for (int j = 0; j < G; ++j) {
-                const int s = g * G + j;
-                if (s >= NS) break;
-                const double* fp = fd + s * NT * 32 + lane;
-#pragma unroll
-                for (int t = 0; t < NT; ++t) dmma_884(acc[t][0], acc[t][1], c2[j], fp[t * 32]);
-                if (lower) {
-                    const double* lp = fl + lower_step_offset(s) * 32 + lane;
-#pragma unroll
-                    for (int t = 0; t <= s / 2; ++t) dmma_884(acc[t][0], acc[t][1], c1[j], lp[t * 32]);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < G; ++j) {
-                c2[j] = n2[j];
-                c1[j] = n1[j];
-            }
-            if (g + 2 < NG) {
-                const double chain = acc[0][0];
-                load_group(g + 2, n2, n1, hold(p2, chain, zero), hold(p1, chain, zero));
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int col = 4 * t + cq;
-            if (live && col < k) D[row + (int64_t)col * ldd] = zmake(acc[t][0], acc[t][1]);
-        }
-    }
-}
-
-// The same product on the FP64 pipes for k > 64: a thread per row, output
-// columns in order, so D may be the same matrix as A1 (column j of the
-// result reads columns l >= j of A1 only) but must not overlap A2.
-__global__ void __launch_bounds__(128)
-rmul_rows_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* __restrict__ A2, int64_t lda2,
-                 int64_t rows, int k, const z64* __restrict__ L, const z64* __restrict__ C, z64 beta, int use_beta) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += stride) {
-        for (int j = 0; j < k; ++j) {
-            z64 acc = use_beta ? zmul(beta, D[r + (int64_t)j * ldd]) : zmake(0.0, 0.0);
-            if (A1)
-                for (int l = j; l < k; ++l) zmac(acc, A1[r + (int64_t)l * lda1], __ldg(L + l + (int64_t)j * k));
-            for (int l = 0; l < k; ++l) zmac(acc, A2[r + (int64_t)l * lda2], __ldg(C + l + (int64_t)j * k));
-            D[r + (int64_t)j * ldd] = acc;
-        }
-    }
-}
-
-template <int NT>
-static int launch_rmul_dmma(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2,
-                            int64_t rows, int k, const double* fdense, const double* flower, z64 beta, int use_beta,
-                            cudaStream_t stream) {
-    const size_t smem = (size_t)(dense_frag_doubles(NT) + (A1 ? lower_frag_doubles(NT) : 0)) * sizeof(double);
-    FB_CUDA(cudaFuncSetAttribute(rmul_dmma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-            "cudaFuncSetAttribute(rmul_dmma_kernel)");
-    int per_sm = 0;
-    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rmul_dmma_kernel<NT>, AD_THREADS, smem),
-            "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) per_sm = 1;
-    const int64_t units = (rows + 7) / 8;
-    int64_t need = (units + AD_THREADS / 32 - 1) / (AD_THREADS / 32);
-    int64_t grid = (int64_t)sm_count() * per_sm;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    rmul_dmma_kernel<NT><<<(unsigned)grid, AD_THREADS, smem, stream>>>(D, ldd, A1, lda1, A2, lda2, rows, k, fdense,
-                                                                       flower, beta, use_beta, 0);
-    FB_LAUNCHED("rmul_dmma_kernel");
-    return FB_OK;
-}
-
-// D <- beta D + A1 L + A2 C with L, C (and their fragments when k <= 64) in
-// the workspace.
-static int rmul_enqueue(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2,
-                        int64_t rows, int k, const z64* L, const z64* C, const double* fdense,
-                        const double* flower, z64 beta, int use_beta, cudaStream_t stream) {
-    if (rows == 0 || k == 0) return FB_OK;
-    if (k <= AD_KMAX) {
-        switch ((k + 3) / 4) {
-#define FB_RM_CASE(n) \
-    case n: return launch_rmul_dmma<n>(D, ldd, A1, lda1, A2, lda2, rows, k, fdense, flower, beta, use_beta, stream);
-            FB_RM_CASE(1) FB_RM_CASE(2) FB_RM_CASE(3) FB_RM_CASE(4) FB_RM_CASE(5) FB_RM_CASE(6)
-            FB_RM_CASE(7) FB_RM_CASE(8) FB_RM_CASE(9) FB_RM_CASE(10) FB_RM_CASE(11) FB_RM_CASE(12)
-            FB_RM_CASE(13) FB_RM_CASE(14) FB_RM_CASE(15) FB_RM_CASE(16)
-#undef FB_RM_CASE
-        }
-    }
-    int64_t grid = (int64_t)sm_count() * 8;
-    int64_t need = (rows + 127) / 128;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    rmul_rows_kernel<<<(unsigned)grid, 128, 0, stream>>>(D, ldd, A1, lda1, A2, lda2, rows, k, L, C, beta, use_beta);
-    FB_LAUNCHED("rmul_rows_kernel");
-    return FB_OK;
 }
 
 // Workspace of the cholqr2! adjoint: six k x k matrices, the fragments, the
@@ -354,8 +141,8 @@ static AdjointLayout adjoint_layout(int64_t N, int k) {
     a.T = off; off += mat;
     a.L = off; off += mat;
     a.C = off; off += mat;
-    a.fdense = off; off += k <= AD_KMAX ? align_up((size_t)dense_frag_doubles(nt) * sizeof(double), 256) : 0;
-    a.flower = off; off += k <= AD_KMAX ? align_up((size_t)lower_frag_doubles(nt) * sizeof(double), 256) : 0;
+    a.fdense = off; off += k <= RM_KMAX ? align_up((size_t)dense_frag_doubles(nt, nt) * sizeof(double), 256) : 0;
+    a.flower = off; off += k <= RM_KMAX ? align_up((size_t)lower_frag_doubles(nt) * sizeof(double), 256) : 0;
     a.gram = off;
     a.gram_bytes = align_up(gram_workspace_size(N, k, k, false), 256);
     off += a.gram_bytes;
@@ -370,7 +157,8 @@ struct ProjectLayout {
 static ProjectLayout project_layout(int k) {
     ProjectLayout p{};
     const size_t mat = align_up((size_t)k * k * sizeof(z64), 256);
-    const size_t frag = k <= AD_KMAX ? align_up((size_t)dense_frag_doubles((k + 3) / 4) * sizeof(double), 256) : 0;
+    const int nt = (k + 3) / 4;
+    const size_t frag = k <= RM_KMAX ? align_up((size_t)dense_frag_doubles(nt, nt) * sizeof(double), 256) : 0;
     p.C1 = 0;
     p.C2 = mat;
     p.f1 = 2 * mat;
@@ -447,8 +235,8 @@ int fb_zcholqr2_adjoint(fb_z128* Ybar, int64_t ldyb, const fb_z128* Y, int64_t l
         reinterpret_cast<const z64*>(R), ldr, reinterpret_cast<const z64*>(Rbar), ldrb, Qb ? mat(lay.X) : nullptr, k,
         mat(lay.Rinv), mat(lay.P), mat(lay.H), mat(lay.T), mat(lay.L), mat(lay.C), fdense, flower);
     FB_LAUNCHED("cholqr2_adjoint_prep_kernel");
-    return rmul_enqueue(reinterpret_cast<z64*>(Ybar), ldyb, Qb, ldqb, Yz, ldy, N, k, mat(lay.L), mat(lay.C), fdense,
-                        flower, zmake(0.0, 0.0), 0, stream);
+    return rmul_enqueue(reinterpret_cast<z64*>(Ybar), ldyb, Qb, ldqb, Yz, ldy, N, k, k, mat(lay.L), k, mat(lay.C), k,
+                        fdense, flower, zmake(0.0, 0.0), 0, stream, nullptr, GATE_ALWAYS);
 }
 
 int fb_zproject_adjoint_workspace_size(int k, size_t* bytes) {
@@ -495,11 +283,11 @@ int fb_zproject_adjoint(fb_z128* Qbar, int64_t ldqb, const fb_z128* GQ, int64_t 
                                                                 hermitian, C1, C2, f1, f2);
     FB_LAUNCHED("project_adjoint_prep_kernel");
     z64* Qb = reinterpret_cast<z64*>(Qbar);
-    FB_TRY(rmul_enqueue(Qb, ldqb, nullptr, 0, reinterpret_cast<const z64*>(GQ), ldgq, N, k, nullptr, C1, f1, nullptr,
-                        zmake(1.0, 0.0), accumulate ? 1 : 0, stream));
+    FB_TRY(rmul_enqueue(Qb, ldqb, nullptr, 0, reinterpret_cast<const z64*>(GQ), ldgq, N, k, k, nullptr, 0, C1, k, f1,
+                        nullptr, zmake(1.0, 0.0), accumulate ? 1 : 0, stream, nullptr, GATE_ALWAYS));
     if (!hermitian)
-        FB_TRY(rmul_enqueue(Qb, ldqb, nullptr, 0, reinterpret_cast<const z64*>(GhQ), ldghq, N, k, nullptr, C2, f2,
-                            nullptr, zmake(1.0, 0.0), 1, stream));
+        FB_TRY(rmul_enqueue(Qb, ldqb, nullptr, 0, reinterpret_cast<const z64*>(GhQ), ldghq, N, k, k, nullptr, 0, C2, k,
+                            f2, nullptr, zmake(1.0, 0.0), 1, stream, nullptr, GATE_ALWAYS));
     return FB_OK;
 }
 

@@ -2,118 +2,82 @@
 // (src/kernels.jl:57-88): dst <- A C. (k <= 64 goes to the tensor-core
 // solvers in fb_trsm_dmma.cu.)
 //
-// Both are row-independent, so a thread owns a row. For k <= 64 the row lives
-// in registers for the whole solve, and the substitution runs right-looking:
-// once column j of the result is known it is subtracted from every later
-// column, which gives the FP64 pipe long runs of independent fused
-// multiply-adds. R sits in shared memory and every thread of a warp reads the
-// same entry at the same time, so each read is one broadcast. Loads and
-// stores of a row are one column at a time across the warp: 32 consecutive
-// rows of a column-major block, 512 contiguous bytes per warp instruction.
-// The grid is persistent (a few CTAs per SM) so R is staged once per CTA.
+// Past 64 columns the solve goes by 64-column blocks: for block b,
+//     Y_b <- Y_b - sum_{c<b} X_c R_cb    (the tensor-core right product of
+//                                         fb_rmul.cuh, one launch per c),
+//     X_b  = Y_b R_bb^-1                 (the k <= 64 solver),
+// so every flop still runs on the FP64 tensor cores. A prep kernel lays out
+// -R_cb as MMA fragments for every pair c < b; each diagonal block gets the
+// k <= 64 solver's own plan and fragments, so its path (one product by the
+// inverse, blocked, or substitution) is chosen for that block alone.
 #include "fb_common.cuh"
+#include "fb_rmul.cuh"
 
 namespace fb {
 
-__device__ __forceinline__ z64 zrecip(z64 d) {
-    double s = 1.0 / fma(d.x, d.x, d.y * d.y);
-    return zmake(d.x * s, -d.y * s);
-}
-
-// The solve goes 16 columns at a time. For block b a thread first takes the
-// finished columns 0..16b-1 of its own row off the block (left-looking: the
-// row is read back, these are values this thread has just written), then
-// solves the block's own 16 x 16 triangle right-looking. Sixteen columns of
-// state keep the thread near 100 registers, so a warp scheduler has several
-// warps to choose from while one waits on memory.
-constexpr int TB = 16;
-
-template <int J>
-__device__ __forceinline__ void solve_block(z64 (&y)[TB], const z64* Rb, int ld, const z64* dinv) {
-    if constexpr (J < TB) {
-        z64 q = zmul(y[J], dinv[J]);
-        y[J] = q;
-#pragma unroll
-        for (int l = J + 1; l < TB; ++l) zmsub(y[l], q, Rb[J * ld + l]);
-        solve_block<J + 1>(y, Rb, ld, dinv);
-    }
-}
-
-// R is staged row-major in shared memory (ld = kp, k rounded up to 16, zero
-// outside the upper triangle and past k; the reciprocal diagonal apart).
-__global__ void __launch_bounds__(128)
-trsm_rows_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k,
-                 const z64* __restrict__ R, int64_t ldr, const ChainStatus* st, int gate) {
-    if (gated_off(st, gate)) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int kp = (k + TB - 1) / TB * TB;
-    z64* Rs = reinterpret_cast<z64*>(smem_raw);
-    z64* dinv = Rs + (size_t)kp * kp;
-    for (int e = threadIdx.x; e < kp * kp; e += blockDim.x) {
-        int j = e / kp, l = e - j * kp;
-        z64 v = zmake(0.0, 0.0);
-        if (j < k && l < k && j < l) v = R[j + (int64_t)l * ldr];
-        Rs[e] = v;
-    }
-    for (int j = threadIdx.x; j < kp; j += blockDim.x)
-        dinv[j] = (j < k) ? zrecip(R[j + (int64_t)j * ldr]) : zmake(0.0, 0.0);
-    __syncthreads();
-
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += stride) {
-        z64* row = Y + r;
-        for (int b0 = 0; b0 < kp; b0 += TB) {
-            z64 y[TB];
-#pragma unroll
-            for (int c = 0; c < TB; ++c) y[c] = (b0 + c < k) ? row[(int64_t)(b0 + c) * ldy] : zmake(0.0, 0.0);
-#pragma unroll 2
-            for (int i = 0; i < b0; ++i) {
-                const z64 q = row[(int64_t)i * ldy];
-                const z64* Ri = Rs + i * kp + b0;
-#pragma unroll
-                for (int c = 0; c < TB; ++c) zmsub(y[c], q, Ri[c]);
-            }
-            solve_block<0>(y, Rs + b0 * kp + b0, kp, dinv + b0);
-#pragma unroll
-            for (int c = 0; c < TB; ++c)
-                if (b0 + c < k) row[(int64_t)(b0 + c) * ldy] = y[c];
-        }
-    }
-}
+constexpr int TB_COLS = 64;  // columns of a block of the blocked solve
 
 int trsm_dmma_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
                       size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate);
-size_t trsm_workspace_bytes(int k);
+size_t trsm_workspace_bytes_small(int k);
+
+static int trsm_blocks(int k) { return (k + TB_COLS - 1) / TB_COLS; }
+static size_t trsm_diag_bytes() { return align_up(trsm_workspace_bytes_small(TB_COLS), 256); }
+static size_t trsm_pair_bytes() { return align_up((size_t)dense_frag_doubles(TB_COLS / 4, TB_COLS / 4) * sizeof(double), 256); }
+
+size_t trsm_workspace_bytes(int k) {
+    if (k <= TB_COLS) return trsm_workspace_bytes_small(k);
+    const size_t nb = trsm_blocks(k);
+    return nb * trsm_diag_bytes() + nb * (nb - 1) / 2 * trsm_pair_bytes();
+}
+
+// Block p = b (b - 1) / 2 + c of the grid lays out -R_cb (64 x width of b).
+__global__ void __launch_bounds__(256)
+trsm_pairs_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, double* frags, size_t pair_doubles,
+                       const ChainStatus* st, int gate) {
+    if (gated_off(st, gate)) return;
+    const int p = blockIdx.x;
+    int b = 1;
+    while ((b + 1) * b / 2 <= p) ++b;
+    const int c = p - b * (b - 1) / 2;
+    const int width = (k - TB_COLS * b) < TB_COLS ? k - TB_COLS * b : TB_COLS;
+    build_dense_frags(frags + p * pair_doubles, R + (int64_t)TB_COLS * c + (int64_t)TB_COLS * b * ldr, ldr, TB_COLS,
+                      width, -1.0);
+}
 
 int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
                  size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate) {
     if (rows == 0 || k == 0) return FB_OK;
-    if (k <= 64) return trsm_dmma_enqueue(Y, ldy, rows, k, R, ldr, workspace, workspace_bytes, stream, st, gate);
-    const int threads = 128;
-    const int kp = (k + TB - 1) / TB * TB;
-    size_t smem = ((size_t)kp * kp + kp) * sizeof(z64);
-    if (smem > 227 * 1024) {
-        set_error(FB_ENOTSUP, "rdiv_upper!: k = %d is past the %d columns whose factor fits in shared memory", k, 112);
-        return FB_ENOTSUP;
+    if (k <= TB_COLS) return trsm_dmma_enqueue(Y, ldy, rows, k, R, ldr, workspace, workspace_bytes, stream, st, gate);
+    if (!workspace || workspace_bytes < trsm_workspace_bytes(k)) {
+        set_error(FB_ENOMEM, "rdiv_upper!: workspace of %zu bytes, need %zu", workspace_bytes, trsm_workspace_bytes(k));
+        return FB_ENOMEM;
     }
-    FB_CUDA(cudaFuncSetAttribute(trsm_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-            "cudaFuncSetAttribute(trsm_rows_kernel)");
-    int per_sm = 0;
-    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsm_rows_kernel, threads, smem),
-            "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) per_sm = 1;
-    int64_t need = (rows + threads - 1) / threads;
-    int64_t grid = (int64_t)sm_count() * per_sm;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    trsm_rows_kernel<<<(unsigned)grid, threads, smem, stream>>>(Y, ldy, rows, k, R, ldr, st, gate);
-    FB_LAUNCHED("trsm_rows_kernel");
+    const int nb = trsm_blocks(k);
+    char* ws = static_cast<char*>(workspace);
+    double* pairs = reinterpret_cast<double*>(ws + (size_t)nb * trsm_diag_bytes());
+    const size_t pair_doubles = trsm_pair_bytes() / sizeof(double);
+    trsm_pairs_prep_kernel<<<nb * (nb - 1) / 2, 256, 0, stream>>>(R, ldr, k, pairs, pair_doubles, st, gate);
+    FB_LAUNCHED("trsm_pairs_prep_kernel");
+    for (int b = 0; b < nb; ++b) {
+        const int width = k - TB_COLS * b < TB_COLS ? k - TB_COLS * b : TB_COLS;
+        z64* Yb = Y + (int64_t)TB_COLS * b * ldy;
+        for (int c = 0; c < b; ++c) {
+            const double* frag = pairs + (size_t)(b * (b - 1) / 2 + c) * pair_doubles;
+            FB_TRY(rmul_enqueue(Yb, ldy, nullptr, 0, Y + (int64_t)TB_COLS * c * ldy, ldy, rows, TB_COLS, width,
+                                nullptr, 0, nullptr, 0, frag, nullptr, zmake(1.0, 0.0), 1, stream, st, gate));
+        }
+        FB_TRY(trsm_dmma_enqueue(Yb, ldy, rows, width, R + (int64_t)TB_COLS * b * (1 + ldr), ldr,
+                                 ws + (size_t)b * trsm_diag_bytes(), trsm_diag_bytes(), stream, st, gate));
+    }
     return FB_OK;
 }
 
-// dst <- A C. A thread owns a row and produces its outputs 16 columns at a
+// dst <- A C. A thread owns a row and produces its outputs TB columns at a
 // time: a loop over the s columns of A (read from the row) accumulates
 // the block against row i of C, staged in shared memory.
+constexpr int TB = 16;
+
 __global__ void __launch_bounds__(128)
 gemm_right_kernel(z64* __restrict__ D, int64_t ldd, const z64* __restrict__ A, int64_t lda,
                   int64_t rows, int s, const z64* __restrict__ C, int64_t ldc, int r) {

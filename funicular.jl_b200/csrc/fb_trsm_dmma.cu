@@ -416,7 +416,7 @@ static int launch_trsm_dmma(z64* Y, int64_t ldy, int64_t rows, int k, const Trsm
     return FB_OK;
 }
 
-size_t trsm_workspace_bytes(int k) {
+size_t trsm_workspace_bytes_small(int k) {
     return k <= TR_KMAX ? (size_t)TR_PLAN_BYTES + (size_t)TR_FRAG_DOUBLES * sizeof(double) : 0;
 }
 
@@ -425,8 +425,9 @@ size_t trsm_workspace_bytes(int k) {
 int trsm_dmma_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
                       size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate) {
     if (k > TR_KMAX) { set_error(FB_ENOTSUP, "trsm_dmma: k = %d is past %d", k, TR_KMAX); return FB_ENOTSUP; }
-    if (!workspace || workspace_bytes < trsm_workspace_bytes(k)) {
-        set_error(FB_ENOMEM, "rdiv_upper!: workspace of %zu bytes, need %zu", workspace_bytes, trsm_workspace_bytes(k));
+    if (!workspace || workspace_bytes < trsm_workspace_bytes_small(k)) {
+        set_error(FB_ENOMEM, "rdiv_upper!: workspace of %zu bytes, need %zu", workspace_bytes,
+                  trsm_workspace_bytes_small(k));
         return FB_ENOMEM;
     }
     TrsmPlan* plan = static_cast<TrsmPlan*>(workspace);

@@ -86,7 +86,8 @@ def test_gram_views(fb, backend, oracle):
         fb.kernels.gram_accumulate(backend, C, Ad, Bd.view(slice(None), slice(0, 2)), 1.0, 0.0)
 
 
-@pytest.mark.parametrize("rows,k", [(7, 5), (1, 1), (129, 16), (1000, 23), (5000, 64), (300, 65), (257, 100)])
+@pytest.mark.parametrize("rows,k", [(7, 5), (1, 1), (129, 16), (1000, 23), (5000, 64), (300, 65), (257, 100),
+                                   (3000, 128), (2001, 129), (1500, 200), (100, 257)])
 def test_rdiv_upper(fb, backend, oracle, rows, k):
     rng = np.random.default_rng(rows + k)
     Y = randmatrix(rng, rows, k)
@@ -206,7 +207,8 @@ def test_cholesky_product(fb, backend, oracle, k):
     np.testing.assert_allclose(Rout.to_host(), expect, rtol=1e-12, atol=1e-12 * np.abs(expect).max())
 
 
-@pytest.mark.parametrize("N,k", [(40, 23), (2 ** 16, 32), (100_000, 64), (5000, 100), (3, 3)])
+@pytest.mark.parametrize("N,k", [(40, 23), (2 ** 16, 32), (100_000, 64), (5000, 100), (3, 3), (200_000, 128),
+                                 (20_000, 150)])
 def test_cholqr2_resident_matches_oracle(fb, backend, oracle, N, k):
     rng = np.random.default_rng(N + k)
     A = randmatrix(rng, N, k)
@@ -318,3 +320,22 @@ def test_rdiv_upper_both_tensor_core_paths(fb, backend, oracle, k, scale):
     cond = np.linalg.norm(R, 1) * np.linalg.norm(np.linalg.inv(R), 1)
     np.testing.assert_allclose(X, expect, rtol=0, atol=1e-14 * cond * np.abs(expect).max())
     assert np.linalg.norm(X @ R - Y) <= 1e-14 * np.linalg.norm(Y) * max(1.0, np.sqrt(cond))
+
+
+@pytest.mark.parametrize("kappa", [1e4, 1e7])
+def test_cholqr2_resident_k128_conditioned(fb, backend, oracle, kappa):
+    # Past 64 columns the triangular solves go by 64-column blocks, each
+    # diagonal block choosing its own path; the result keeps the accuracy
+    # targets of the plain form.
+    rng = np.random.default_rng(int(np.log10(kappa)) + 128)
+    N, k = 100_000, 128
+    A = conditioned(rng, N, k, kappa)
+    Y = backend.todevice(A)
+    R = nanbuffer(backend, (k, k))
+    passes, _ = fb.kernels.cholqr2_resident(backend, Y, R)
+    Q, Rh = Y.to_host(), R.to_host()
+    Qo = A.copy(order="F")
+    _, passes_o = oracle.cholqr2(Qo)
+    assert passes == passes_o
+    assert oracle.orthogonality_error(Q) <= 1e-12
+    assert oracle.reconstruction_error(A, Q, Rh) <= 1e-13

@@ -78,8 +78,8 @@ __host__ __device__ inline int off_tile_index(int nt, int ti, int tj) {
     return nt + ti * (2 * nt - ti - 1) / 2 + (tj - ti - 1);
 }
 
-// Consumer warps per block count: at most 16 with two blocks a warp, 12 with
-// three, 8 with eight. Fewer warps leave each more registers.
+// Consumer warps per block count: at most 16 with two or four blocks a warp,
+// 12 with three, 8 with eight. Fewer warps leave each more registers.
 template <int PPW>
 __global__ void __launch_bounds__(PPW >= 8 ? 9 * 32 : PPW == 3 ? 13 * 32 : G_MAX_WARPS * 32, 1)
 gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -163,6 +163,16 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 #pragma unroll
     for (int i = 0; i < PPW; ++i) {
         const int slot = warp * PPW + i;
+        if constexpr (PPW == 4) {
+            // A full 64 x 64 tile: warp w owns half of block row w / 2. The
+            // offsets below are then one base plus constants, which keeps the
+            // 16-warp kernel inside its register budget.
+            valid[i] = true;
+            bi[i] = warp >> 1;
+            bj[i] = 4 * (warp & 1) + i;
+            dpair[i] = false;
+            continue;
+        }
         valid[i] = ln.pi[slot] >= 0;
         bi[i] = valid[i] ? ln.pi[slot] : ln.pi[0];
         bj[i] = valid[i] ? ln.pj[slot] : ln.pj[0];
@@ -343,10 +353,18 @@ static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian, int cta
     sh.nt_b = (kB + sh.tw_b - 1) / sh.tw_b;
     sh.hermitian = hermitian;
     sh.ntiles = hermitian ? sh.nt_a * (sh.nt_a + 1) / 2 : sh.nt_a * sh.nt_b;
-    int largest_launch = hermitian ? (sh.nt_a > 1 ? sh.nt_a * (sh.nt_a - 1) / 2 : 1) : sh.ntiles;
-    if (hermitian && sh.nt_a > largest_launch) largest_launch = sh.nt_a;
+    // Chunks along the rows: enough for the launch with fewer tiles to fill
+    // the GPU by itself (the other then runs in whole or near-whole waves).
+    // A Hermitian Gram of two tile columns has two diagonal tiles but one
+    // off-diagonal tile; sizing for the larger launch would leave half the
+    // SMs idle in the smaller.
+    int smallest_launch = sh.ntiles;
+    if (hermitian && sh.nt_a > 1) {
+        const int off = sh.nt_a * (sh.nt_a - 1) / 2;
+        smallest_launch = off < sh.nt_a ? off : sh.nt_a;
+    }
     const int64_t stages = (rows + GS_ROWS - 1) / GS_ROWS;
-    int64_t target = (int64_t)sm_count() * ctas_per_sm / largest_launch;
+    int64_t target = (int64_t)sm_count() * ctas_per_sm / smallest_launch;
     if (target < 1) target = 1;
     if (target > stages) target = stages;
     if (target < 1) target = 1;
@@ -416,10 +434,12 @@ static GramLaunch gram_launch(const GramShape& sh, bool diag) {
         ln.ntiles = sh.hermitian ? sh.nt_a * (sh.nt_a - 1) / 2 : sh.nt_a * sh.nt_b;
         ln.npairs = ln.nb_a * ln.nb_b;
     }
-    // Blocks per warp: three (at most 12 consumer warps), two (at most 16) or
-    // eight (at most 8), whichever leaves no warp with a block to spare.
+    // Blocks per warp: three (at most 12 consumer warps), two (at most 16),
+    // four (a full 64 x 64 tile: 16 warps, each half a block row) or eight
+    // (at most 8), whichever leaves no warp with a block to spare.
     if (ln.npairs % 3 == 0 && ln.npairs <= 36) ln.ppw = 3;
     else if (ln.npairs <= 32) ln.ppw = 2;
+    else if (ln.npairs == 64) ln.ppw = 4;
     else ln.ppw = 8;
     ln.consumers = (ln.npairs + ln.ppw - 1) / ln.ppw;
     build_pair_table(ln);
@@ -495,6 +515,7 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
             switch (ln.ppw) {
                 case 2: status = launch_gram_dmma<2>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
                 case 3: status = launch_gram_dmma<3>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
+                case 4: status = launch_gram_dmma<4>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
                 default: status = launch_gram_dmma<8>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
             }
             FB_TRY(status);
@@ -518,7 +539,7 @@ size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian) {
 // GPU that loads the library holds these bytes until the process exits. The
 // partial tiles it holds are written by each call before that call reads
 // them, so nothing in it has to start at zero.
-constexpr size_t GRAM_STATIC_SCRATCH_BYTES = (size_t)16 << 20;
+constexpr size_t GRAM_STATIC_SCRATCH_BYTES = (size_t)32 << 20;
 static __device__ __align__(256) unsigned char g_gram_static_scratch[GRAM_STATIC_SCRATCH_BYTES];
 
 // The device address of g_gram_static_scratch on the current device. Host

@@ -153,9 +153,9 @@ int fb_zgram(fb_z128* C, int64_t ldc,
  * cannot afford cudaMalloc's implicit device synchronization in the middle of
  * a pipelined sweep. This entry point computes the same thing as fb_zgram,
  * with the same bits, but keeps its partial tiles in a scratch array built
- * into the library: 16 MiB, held on every GPU that loads the library until
+ * into the library: 32 MiB, held on every GPU that loads the library until
  * the process exits. Shapes whose scratch would not fit in it
- * (fb_zgram_workspace_size above 16 MiB, which takes many 64 x 64 output
+ * (fb_zgram_workspace_size above 32 MiB, which takes many 64 x 64 output
  * tiles: every Gram of at most 128 columns fits) are refused with FB_ENOMEM
  * before anything is enqueued. The first call on each device looks up the array's device
  * address; make it before any stream capture begins. All calls share the one

@@ -63,10 +63,10 @@ def test_static_scratch_matches_the_workspace_entry_point(fb, backend, oracle, r
 
 
 def test_static_scratch_refuses_shapes_that_do_not_fit(fb, backend):
-    rows, k = 100_000, 192
+    rows, k = 100_000, 448
     need = ctypes.c_size_t(0)
     fb._lib.call("fb_zgram_workspace_size", ctypes.c_int64(rows), k, k, 1, ctypes.byref(need))
-    assert need.value > 16 << 20  # a Hermitian 192 x 192 Gram over 1e5 rows: 6 tiles x 49 chunks on a B200
+    assert need.value > 32 << 20  # a Hermitian 448 x 448 Gram over 1e5 rows: 28 tiles x 21 chunks on a B200
     A = backend.alloc_device(np.complex128, (rows, k))
     C = backend.alloc_device(np.complex128, (k, k))
     lib = fb._lib.load()
@@ -74,5 +74,5 @@ def test_static_scratch_refuses_shapes_that_do_not_fit(fb, backend):
     status = lib.fb_zgram_static(_vp(C.ptr), C.ld, _vp(A.ptr), A.ld, _vp(A.ptr), A.ld, rows, k, k,
                                  fb._lib.z128(1.0), fb._lib.z128(0.0), None)
     assert status == fb._lib.FB_ENOMEM
-    assert "16777216" in fb._lib.last_error()
+    assert "33554432" in fb._lib.last_error()
     assert fb._lib.kernel_launches() == before

@@ -1,27 +1,35 @@
 // The tensor-core right product D <- beta D + A1 L + A2 C (fb_rmul.cuh).
 //
-// A warp owns 8 rows at a time. It streams their entries one k-step (two
-// complex columns) at a time, loading each entry of A1 and A2 once, and keeps
-// every output n-tile in its accumulators, so each output entry is written
-// once. The loads run two groups of four k-steps ahead of the products; the
-// group after that waits for the products of the current one, which bounds
-// the registers the prefetch holds.
+// A team of one or two warps owns 8 rows at a time, each warp a contiguous
+// share of the output n-tiles. A warp streams the rows' entries one k-step
+// (two complex columns) at a time, loading each entry of A1 and A2 once (the
+// second warp of a team finds them in L1), and keeps its n-tiles in its
+// accumulators, so each output entry is written once. The loads run two
+// groups of four k-steps ahead of the products; the group after that waits for
+// the products of the current one, which bounds the registers the prefetch
+// holds.
 #include "fb_rmul.cuh"
 #include "fb_tma.cuh"
 
 namespace fb {
 
-constexpr int RM_THREADS = 256;
+constexpr int RM_THREADS = 512;
+// Warps that share one 8-row unit, each taking a contiguous share of the
+// output n-tiles: wide factors split in two, which halves the accumulators a
+// thread holds and lets 16 warps run on an SM instead of 8.
+__host__ __device__ constexpr int rm_split(int ntn) { return ntn >= 8 ? 2 : 1; }
 
 template <int NTK, int NTN>
 __global__ void __launch_bounds__(RM_THREADS, 1)
 rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2, int64_t rows,
                  int K, int n, const double* __restrict__ gdense, const double* __restrict__ glower, z64 beta,
-                 int use_beta, int zero, const ChainStatus* st, int gate) {
+                 int use_beta, int zero, int inplace, const ChainStatus* st, int gate) {
     if (gated_off(st, gate)) return;
-    constexpr int NS = 2 * NTK;         // k-steps
-    constexpr int NT = NTN;             // output n-tiles
-    constexpr int G = 4;                // k-steps whose inputs are loaded together
+    constexpr int NS = 2 * NTK;               // k-steps
+    constexpr int NT = NTN;                   // output n-tiles
+    constexpr int SPLIT = rm_split(NTN);      // warps sharing one 8-row unit
+    constexpr int NH = (NT + SPLIT - 1) / SPLIT;  // n-tiles of one warp
+    constexpr int G = 4;                      // k-steps whose inputs are loaded together
     constexpr int NG = (NS + G - 1) / G;
     constexpr bool SQUARE = NTK == NTN;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -43,8 +51,10 @@ rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
     const int rr = lane >> 2, cq = lane & 3, acol = cq >> 1;
     const int apart = lane & 1;
     const int64_t units = (rows + 7) / 8;
-    const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; u < units; u += warps_total) {
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const int t0 = (int)(gw % SPLIT) * NH;    // this warp's first n-tile
+    const int64_t teams = (int64_t)gridDim.x * (blockDim.x >> 5) / SPLIT;
+    for (int64_t u = gw / SPLIT; u < units; u += teams) {
         const int64_t row = u * 8 + rr;
         const bool live = row < rows;
         const int64_t r0 = live ? row : 0;
@@ -59,20 +69,22 @@ rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
                 b1[j] = (ok && lower) ? reinterpret_cast<const double*>(p1 + (int64_t)col * lda1)[apart] : 0.0;
             }
         };
-        double acc[NT][2];
+        double acc[NH][2];
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int col = 4 * t + cq;
+        for (int h = 0; h < NH; ++h) {
+            const int col = 4 * (t0 + h) + cq;
             z64 d = zmake(0.0, 0.0);
             if (use_beta && live && col < n) d = zmul(beta, D[r0 + (int64_t)col * ldd]);
-            acc[t][0] = d.x;
-            acc[t][1] = d.y;
+            acc[h][0] = d.x;
+            acc[h][1] = d.y;
         }
         const z64* p2 = A2 + r0;
         const z64* p1 = lower ? A1 + r0 : A2 + r0;
         double c2[G], c1[G], n2[G], n1[G];
         load_group(0, c2, c1, p2, p1);
         load_group(1, n2, n1, p2, p1);
+        // Two groups of loads in flight: group g + 2 is issued once group
+        // g's products are done, so its registers are not held any longer.
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
 #pragma unroll
@@ -82,13 +94,15 @@ rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
                 // This step's fragments are read once the previous step's
                 // first product is done, not hoisted further ahead.
                 const double step_chain = acc[0][0];
-                const double* fp = hold(fd + s * NT * 32 + lane, step_chain, zero);
+                const double* fp = hold(fd + (s * NT + t0) * 32 + lane, step_chain, zero);
 #pragma unroll
-                for (int t = 0; t < NT; ++t) dmma_884(acc[t][0], acc[t][1], c2[j], fp[t * 32]);
+                for (int h = 0; h < NH; ++h)
+                    if (SPLIT == 1 || t0 + h < NT) dmma_884(acc[h][0], acc[h][1], c2[j], fp[h * 32]);
                 if (SQUARE && lower) {
-                    const double* lp = hold(fl + lower_step_offset(s) * 32 + lane, step_chain, zero);
+                    const double* lp = hold(fl + (lower_step_offset(s) + t0) * 32 + lane, step_chain, zero);
 #pragma unroll
-                    for (int t = 0; t <= s / 2 && t < NT; ++t) dmma_884(acc[t][0], acc[t][1], c1[j], lp[t * 32]);
+                    for (int h = 0; h < NH; ++h)
+                        if (t0 + h <= s / 2 && t0 + h < NT) dmma_884(acc[h][0], acc[h][1], c1[j], lp[h * 32]);
                 }
             }
 #pragma unroll
@@ -101,10 +115,13 @@ rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
                 load_group(g + 2, n2, n1, hold(p2, chain, zero), hold(p1, chain, zero));
             }
         }
+        // When D is one of the inputs, the other warp of the team may still be
+        // reading these rows: both finish reading before either writes.
+        if (SPLIT > 1 && inplace) asm volatile("bar.sync %0, %1;" ::"r"(1 + warp / SPLIT), "r"(32 * SPLIT) : "memory");
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int col = 4 * t + cq;
-            if (live && col < n) D[row + (int64_t)col * ldd] = zmake(acc[t][0], acc[t][1]);
+        for (int h = 0; h < NH; ++h) {
+            const int col = 4 * (t0 + h) + cq;
+            if (live && col < n && t0 + h < NT) D[row + (int64_t)col * ldd] = zmake(acc[h][0], acc[h][1]);
         }
     }
 }
@@ -142,12 +159,14 @@ static int launch_rmul_dmma(z64* D, int64_t ldd, const z64* A1, int64_t lda1, co
             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) per_sm = 1;
     const int64_t units = (rows + 7) / 8;
-    int64_t need = (units + RM_THREADS / 32 - 1) / (RM_THREADS / 32);
+    const int teams_per_cta = RM_THREADS / 32 / rm_split(NTN);
+    int64_t need = (units + teams_per_cta - 1) / teams_per_cta;
     int64_t grid = (int64_t)sm_count() * per_sm;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
+    const int inplace = (D == A1 || D == A2) ? 1 : 0;
     rmul_dmma_kernel<NTK, NTN><<<(unsigned)grid, RM_THREADS, smem, stream>>>(
-        D, ldd, lower ? A1 : nullptr, lda1, A2, lda2, rows, K, n, fdense, flower, beta, use_beta, 0, st, gate);
+        D, ldd, lower ? A1 : nullptr, lda1, A2, lda2, rows, K, n, fdense, flower, beta, use_beta, 0, inplace, st, gate);
     FB_LAUNCHED("rmul_dmma_kernel");
     return FB_OK;
 }

@@ -61,7 +61,9 @@ def parse_args():
                    help="rows of the k = 128 configuration (0 skips it)")
     p.add_argument("--adjoint-N", type=int, default=1 << 22,
                    help="rows of the differentiation workload (0 skips it)")
-    p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace"), default=None,
+    p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace",
+                                      "cholqr2", "cholqr2_adjoint", "project_adjoint", "hband", "adjoint_step"),
+                   default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
     return p.parse_args()
@@ -322,6 +324,65 @@ def run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, f
                             "orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                             "reconstruction_rel": recon})
         del Yt, Y
+    return out
+
+
+def run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, barrier):
+    """The wide configuration's storage comparison, end to end through the
+    public API on page-locked host panels (N = args.wide_N, k = 128,
+    kappa = 1e7): cholqr2 with ComplexF64 host storage, and the shifted
+    CholeskyQR3 (cholqr3) with a ComplexF32 host tier, which halves the bytes
+    that cross the bus. Both run the device-resident FP64 chain; each call
+    uploads the panels (widened on the device), orthonormalizes, and writes
+    Q back (narrowed on the device). Accuracy of what the panels hold after
+    the call is measured on the device against the stored input."""
+    N, k = args.wide_N, 128
+    Yt0 = build_workload(fb, backend, torch, device, N, k, seed=0xC37, kappa=1e7)
+    Yhost = np.asfortranarray(wrap(fb, Yt0, N, k).to_host())
+    del Yt0
+    out = {"workload": f"N={N}, k={k}, kappa=1e7, device-resident chain, host panels page-locked", "runs": []}
+    for storage, fn, name in ((np.complex128, fb.cholqr2, "cholqr2, ComplexF64 storage"),
+                              (np.complex64, fb.cholqr3, "shifted cholqr3, ComplexF32 storage")):
+        itemsize = np.dtype(storage).itemsize
+        nbytes = N * k * itemsize
+        plan = fb.ResidencyPlan(device_budget=N * k * 16 + 8 * fb.GiB, host_budget=nbytes + 64 * 2 ** 20,
+                                backend=backend, panel_width=32,
+                                host_eltype=None if storage == np.complex128 else storage)
+        Ypm = fb.PanelMatrix.from_array(Yhost, plan=plan)
+        # The stored input (rounded to the storage eltype), widened on the device.
+        q = backend.make_queue()
+        Reft = torch.empty((k, N), dtype=torch.complex128, device=device)
+        fb.panels.to_device(Ypm, wrap(fb, Reft, N, k), q)
+        backend.sync_queue(q)
+        times = []
+        for i in range(3):
+            if i:
+                Ypm.copy_from(Yhost)
+            barrier()
+            t0 = time.perf_counter()
+            R = fn(Ypm, resident=True)
+            times.append(time.perf_counter() - t0)
+        # Accuracy of the panels' Q (in their storage precision) in FP64.
+        Qt = torch.empty_like(Reft)
+        Qd = wrap(fb, Qt, N, k)
+        fb.panels.to_device(Ypm, Qd, q)
+        backend.sync_queue(q)
+        G = backend.alloc_device(np.complex128, (k, k))
+        fb.kernels.gram_accumulate(backend, G, Qd, Qd, 1.0, 0.0)
+        orth = float(np.linalg.norm(G.to_host() - np.eye(k)))
+        QRt = torch.empty_like(Reft)
+        fb.kernels.rightmul_gemm(backend, wrap(fb, QRt, N, k), Qd, backend.todevice(np.asfortranarray(R)))
+        backend.sync_all()
+        QRt.sub_(Reft)
+        recon = float(torch.linalg.vector_norm(QRt).item() / torch.linalg.vector_norm(Reft).item())
+        del Qt, Qd, QRt, Reft
+        ms = max_over_ranks(1e3 * sum(times[1:]) / len(times[1:]))
+        out["runs"].append({"call": name, "storage": np.dtype(storage).name, "ms_per_call": ms,
+                            "bus_bytes_per_call": 2 * nbytes, "value": world * alg_bytes(N, k) / (ms * 1e-3) / 1e9,
+                            "unit": UNIT, "orthogonality_fro": orth, "reconstruction_rel": recon,
+                            "clock": "host wall clock around the synchronous call, 2 calls after one warm-up"})
+        fb.free(Ypm)
+        del Ypm, plan
     return out
 
 
@@ -697,6 +758,8 @@ def run_ours(args):
 
     wide = (run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak)
             if args.wide_N > 0 else None)
+    if wide is not None and args.e2e_steps > 0:
+        wide["storage"] = run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, barrier)
     adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.adjoint_N > 0 else None)
     if adjoint is not None:
@@ -781,6 +844,8 @@ def run_only(args):
     backend = fb.B200Backend(0)
     if args.only == "laplace":
         return run_only_laplace(args, fb, backend, torch, device)
+    if args.only in ("cholqr2_adjoint", "project_adjoint", "hband", "adjoint_step"):
+        return run_only_adjoint(args, fb, backend, torch, device)
     Yt = build_workload(fb, backend, torch, device, N, k, seed=0xDEADBEEF)
     Y = wrap(fb, Yt, N, k)
     # The first pass's factor: the Cholesky factor of Y^H Y (Y is Yt^T).
@@ -797,6 +862,7 @@ def run_only(args):
         "trsm_blocked": lambda: fb.kernels.rdiv_upper(backend, Y, R1),
         "trsm_inverse": lambda: fb.kernels.rdiv_upper(backend, Y, Rid),
         "ghost_fill": lambda: fb.kernels.ghost_fill(backend, Y, 0, 0, 0xDEADBEEF, np.complex128),
+        "cholqr2": lambda: fb.kernels.cholqr2_resident(backend, Y, Gd, wait=False),
     }[args.only]
     for _ in range(args.warmup):
         backend.submit(queue, launch)
@@ -811,6 +877,61 @@ def run_only(args):
     torch.cuda.nvtx.range_pop()
     b.synchronize()
     print(json.dumps({"only": args.only, "N": N, "k": k, "steps": args.steps,
+                      "ms_per_launch": a.elapsed_time(b) / args.steps}), flush=True)
+    return 0
+
+
+def run_only_adjoint(args, fb, backend, torch, device):
+    """The differentiation kernels on N = args.N rows, k = args.k, inputs
+    filled by the ghost generator: `cholqr2_adjoint` (cross Gram, prep, fused
+    product), `project_adjoint` (Hermitian G), `hband` (G Q with kd = 64), or
+    `adjoint_step` (the whole forward pass and both pullbacks of the
+    differentiation workload)."""
+    N, k, kd = args.N, args.k, 64
+    alloc = lambda r, c: backend.alloc_device(np.complex128, (r, c))
+    Y, Qbar, GQ, Q = alloc(N, k), alloc(N, k), alloc(N, k), alloc(N, k)
+    R, S = alloc(k, k), alloc(k, k)
+    fb.kernels.ghost_fill(backend, Y, 0, 0, 0xC5, np.complex128)
+    fb.kernels.ghost_fill(backend, Qbar, 0, 0, 0xC6, np.complex128)
+    fb.device_api.copy_region(Q, Y, None)
+    fb.kernels.cholqr2_resident(backend, Q, R)
+    G = fb.HermitianBand.ghost(backend, N, kd, seed=0xC7, scale=float(np.sqrt(N / ((2 * kd + 1) * k))))
+    G.apply(backend, GQ, Q)
+    fb.kernels.gram_accumulate(backend, S, Q, GQ, 2.0, 0.0)
+    backend.sync_all()
+    Ybar = alloc(N, k)
+    K = fb.kernels
+
+    def step():
+        fb.device_api.copy_region(Q, Y, queue)
+        K.cholqr2_resident(backend, Q, R, wait=False)
+        G.apply(backend, GQ, Q)
+        K.gram_accumulate(backend, S, Q, GQ, 2.0, 0.0)
+        fb.device_api.copy_region(Ybar, Qbar, queue)
+        K.project_adjoint(backend, Ybar, GQ, S, None, accumulate=True)
+        K.cholqr2_adjoint(backend, Ybar, Y, R, Ybar, None)
+
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    launch = {
+        "cholqr2_adjoint": lambda: K.cholqr2_adjoint(backend, Ybar, Y, R, Qbar, None),
+        "project_adjoint": lambda: K.project_adjoint(backend, Ybar, GQ, S, None, accumulate=True),
+        "hband": lambda: G.apply(backend, GQ, Q),
+        "adjoint_step": step,
+    }[args.only]
+    for _ in range(args.warmup):
+        backend.submit(queue, launch)
+    backend.sync_queue(queue)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("only")
+    a.record(stream)
+    for _ in range(args.steps):
+        backend.submit(queue, launch)
+    b.record(stream)
+    torch.cuda.nvtx.range_pop()
+    b.synchronize()
+    print(json.dumps({"only": args.only, "N": N, "k": k, "kd": kd, "steps": args.steps,
                       "ms_per_launch": a.elapsed_time(b) / args.steps}), flush=True)
     return 0
 

@@ -18,7 +18,7 @@ from .plan import (GiB, ResidencyPlan, choose_panel_width, row_block_height, dev
 from .panels import PanelMatrix, free
 from .executor import (sweep, foreachpanel, readpanels, writepanels, updatepanels, PanelSteps, RowSteps,
                        rowtraversal)
-from .panelblas import (gram, panelmul, cholqr2, project, rightmul, DenseOperator, ColumnOperator,
+from .panelblas import (gram, panelmul, cholqr2, cholqr3, project, rightmul, DenseOperator, ColumnOperator,
                         DeviceOperator, Laplacian7, HermitianBand, cholesky_upper)
 from .ghosts import GhostPanels, isghost
 from . import autodiff
@@ -29,6 +29,6 @@ __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceE
            "kernels", "LIBRARY_PATH", "GiB", "ResidencyPlan", "choose_panel_width", "row_block_height",
            "device_bytes_allocated", "host_bytes_reserved", "host_bytes_in_use", "host_bytes_free",
            "PanelMatrix", "free", "sweep", "foreachpanel", "readpanels", "writepanels", "updatepanels",
-           "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "project", "rightmul",
+           "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "cholqr3", "project", "rightmul",
            "DenseOperator", "ColumnOperator", "DeviceOperator", "Laplacian7", "HermitianBand", "cholesky_upper", "GhostPanels", "isghost",
            "autodiff", "rrule"]

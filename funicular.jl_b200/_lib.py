@@ -121,6 +121,9 @@ SIGNATURES = {
     "fb_zproject_adjoint_workspace_size": [_int, _psz],
     "fb_zproject_adjoint": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, _vp, _sz, _vp],
     "fb_zhband_apply": [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, _vp],
+    "fb_zcholqr3_shifted": [_vp, _i64, _i64, _int, _vp, _i64, ctypes.c_double, _pint, _pint, _vp, _sz, _vp],
+    "fb_zpotrf_forced_shift": [_vp, _i64, _vp, _i64, _int, _i64, _vp, _i64, _vp, _i64, ctypes.c_double, _pdbl,
+                               _vp, _sz, _vp],
 }
 _RESTYPES = {"fb_last_error": ctypes.c_char_p, "fb_abi_version": ctypes.c_int,
              "fb_kernel_launches": ctypes.c_uint64}

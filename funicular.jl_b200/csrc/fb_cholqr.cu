@@ -29,7 +29,7 @@ int ozaki_gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, int64_t r
                        int gate);
 int potrf_enqueue(const z64* G, int64_t ldg, int k, int64_t N, z64* U, int64_t ldu,
                   const z64* Rin, int64_t ldrin, z64* Rout, int64_t ldrout, z64* gwork,
-                  ChainStatus* st, int pass, int gate, cudaStream_t stream);
+                  ChainStatus* st, int pass, int gate, cudaStream_t stream, double forced_u);
 
 struct CholqrLayout {
     size_t status, G, U, Ra, Rb, gwork, trsm, gram, total;
@@ -85,7 +85,7 @@ int fb_zcholqr2_workspace_size(int64_t N, int k, size_t* bytes) {
 // status block (a batch keeps one status per instance and shares the rest).
 static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info,
                          int* passes, void* workspace, size_t workspace_bytes, fb_queue_t queue, bool tensor,
-                         ChainStatus* status = nullptr) {
+                         ChainStatus* status = nullptr, double forced_u = 0.0) {
     if (N < 1 || k < 1) {
         set_error(FB_EINVAL, "cholqr2!: N and k must be positive, got N=%lld, k=%d", (long long)N, k);
         return FB_EINVAL;
@@ -128,7 +128,10 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
         else
             FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st,
                                 gate));
-        FB_TRY(potrf_enqueue(G, k, k, N, U, k, rin[pass], k, rout[pass], k, gwork, st, pass, gate, stream));
+        // The shifted CholeskyQR3 shifts pass 1 unconditionally; that marks
+        // the pass as shifted, so the third pass runs and R = R3 R2 R1.
+        FB_TRY(potrf_enqueue(G, k, k, N, U, k, rin[pass], k, rout[pass], k, gwork, st, pass, gate, stream,
+                             pass == 1 ? forced_u : 0.0));
         FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, trsm_ws, trsm_bytes, stream, st, gate));
     }
     int blocks = (int)((int64_t)k * k + 255) / 256;
@@ -150,6 +153,16 @@ static size_t batch_status_bytes(int count) { return align_up((size_t)count * si
 int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
                 void* workspace, size_t workspace_bytes, fb_queue_t queue) {
     return cholqr2_chain(Y, ldy, N, k, R, ldr, info, passes, workspace, workspace_bytes, queue, false);
+}
+
+int fb_zcholqr3_shifted(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, double unit_roundoff,
+                        int* info, int* passes, void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    if (!(unit_roundoff > 0.0 && unit_roundoff < 1.0)) {
+        set_error(FB_EINVAL, "fb_zcholqr3_shifted: the unit roundoff must lie in (0, 1), got %g", unit_roundoff);
+        return FB_EINVAL;
+    }
+    return cholqr2_chain(Y, ldy, N, k, R, ldr, info, passes, workspace, workspace_bytes, queue, false, nullptr,
+                         unit_roundoff);
 }
 
 int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,

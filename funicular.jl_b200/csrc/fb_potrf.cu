@@ -8,6 +8,12 @@
 // pivot is not > 0 (this also catches NaN). On failure the matrix is reloaded
 // with s = 11 N k eps(Float64) ||G||_F added to the diagonal and factored
 // again; a second failure is reported, not shifted further.
+//
+// The shifted CholeskyQR3 of Fukaya, Kannan, Nakatsukasa, Zhang and Yamamoto
+// (SIAM J. Sci. Comput. 2020) shifts its first pass unconditionally: with a
+// unit roundoff u > 0 the kernel factors G + s I once, s = 11 (N k + k (k+1))
+// u ||G||_F (||G||_F bounds ||Y||_2^2 from above, which keeps s inside the
+// range the analysis allows for the condition numbers it targets).
 #include "fb_common.cuh"
 
 namespace fb {
@@ -39,7 +45,7 @@ __global__ void __launch_bounds__(POTRF_THREADS, 1)
 potrf_kernel(const z64* __restrict__ G, int64_t ldg, int k, int64_t N,
              z64* __restrict__ U, int64_t ldu, const z64* __restrict__ Rin, int64_t ldrin,
              z64* __restrict__ Rout, int64_t ldrout, z64* __restrict__ gwork,
-             ChainStatus* st, int pass, int gate) {
+             ChainStatus* st, int pass, int gate, double forced_u) {
     if (gated_off(st, gate)) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_scratch[33];
@@ -63,7 +69,12 @@ potrf_kernel(const z64* __restrict__ G, int64_t ldg, int k, int64_t N,
     bool shifted = false;
     double shift = 0.0;
     bool ok = false;
-    for (int attempt = 0; attempt < 2 && !ok; ++attempt) {
+    if (forced_u > 0.0) {
+        shifted = true;
+        shift = 11.0 * ((double)N * (double)k + (double)k * (double)(k + 1)) * forced_u * gnorm;
+    }
+    const int attempts = forced_u > 0.0 ? 1 : 2;
+    for (int attempt = 0; attempt < attempts && !ok; ++attempt) {
         if (attempt == 1) {
             shifted = true;
             shift = 11.0 * (double)N * (double)k * 2.220446049250313e-16 * gnorm;
@@ -141,14 +152,14 @@ size_t potrf_gwork_bytes(int k) { return k > POTRF_SMEM_MAX_K ? (size_t)k * k * 
 
 int potrf_enqueue(const z64* G, int64_t ldg, int k, int64_t N, z64* U, int64_t ldu,
                   const z64* Rin, int64_t ldrin, z64* Rout, int64_t ldrout, z64* gwork,
-                  ChainStatus* st, int pass, int gate, cudaStream_t stream) {
+                  ChainStatus* st, int pass, int gate, cudaStream_t stream, double forced_u) {
     size_t smem = k <= POTRF_SMEM_MAX_K ? (size_t)k * k * sizeof(z64) : 0;
     if (smem > 0) {
         FB_CUDA(cudaFuncSetAttribute(potrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "cudaFuncSetAttribute(potrf_kernel)");
     }
     potrf_kernel<<<1, POTRF_THREADS, smem, stream>>>(G, ldg, k, N, U, ldu, Rin, ldrin, Rout, ldrout, gwork, st,
-                                                     pass, gate);
+                                                     pass, gate, forced_u);
     FB_LAUNCHED("potrf_kernel");
     return FB_OK;
 }
@@ -165,9 +176,10 @@ int fb_zpotrf_workspace_size(int k, size_t* bytes) {
     return FB_OK;
 }
 
-int fb_zpotrf_shifted(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, int k, int64_t N,
+static int potrf_call(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, int k, int64_t N,
                       const fb_z128* Rin, int64_t ldrin, fb_z128* Rout, int64_t ldrout,
-                      int* shifted, double* shift, void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+                      int* shifted, double* shift, void* workspace, size_t workspace_bytes, fb_queue_t queue,
+                      double forced_u) {
     if (k < 0 || N < 0) { set_error(FB_EINVAL, "fb_zpotrf_shifted: negative size"); return FB_EINVAL; }
     if (k == 0) {
         if (shifted) *shifted = 0;
@@ -195,7 +207,7 @@ int fb_zpotrf_shifted(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, in
     FB_CUDA(cudaMemsetAsync(st, 0, sizeof(ChainStatus), stream), "cudaMemsetAsync");
     FB_TRY(potrf_enqueue(reinterpret_cast<const z64*>(G), ldg, k, N, reinterpret_cast<z64*>(U), ldu,
                          reinterpret_cast<const z64*>(Rin), ldrin, reinterpret_cast<z64*>(Rout), ldrout, gwork, st,
-                         1, GATE_ALWAYS, stream));
+                         1, GATE_ALWAYS, stream, forced_u));
     ChainStatus host{};
     FB_CUDA(cudaMemcpyAsync(&host, st, sizeof host, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync");
     FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
@@ -210,6 +222,24 @@ int fb_zpotrf_shifted(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, in
         return FB_ENOTSPD;
     }
     return FB_OK;
+}
+
+int fb_zpotrf_shifted(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, int k, int64_t N,
+                      const fb_z128* Rin, int64_t ldrin, fb_z128* Rout, int64_t ldrout,
+                      int* shifted, double* shift, void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    return potrf_call(U, ldu, G, ldg, k, N, Rin, ldrin, Rout, ldrout, shifted, shift, workspace, workspace_bytes,
+                      queue, 0.0);
+}
+
+int fb_zpotrf_forced_shift(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg, int k, int64_t N,
+                           const fb_z128* Rin, int64_t ldrin, fb_z128* Rout, int64_t ldrout, double unit_roundoff,
+                           double* shift, void* workspace, size_t workspace_bytes, fb_queue_t queue) {
+    if (!(unit_roundoff > 0.0 && unit_roundoff < 1.0)) {
+        set_error(FB_EINVAL, "fb_zpotrf_forced_shift: the unit roundoff must lie in (0, 1), got %g", unit_roundoff);
+        return FB_EINVAL;
+    }
+    return potrf_call(U, ldu, G, ldg, k, N, Rin, ldrin, Rout, ldrout, nullptr, shift, workspace, workspace_bytes,
+                      queue, unit_roundoff);
 }
 
 }  // extern "C"

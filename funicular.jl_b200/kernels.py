@@ -124,10 +124,13 @@ def rightmul_gemm(backend, dst: DeviceMatrix, A: DeviceMatrix, C: DeviceMatrix) 
 
 
 def cholesky_upper_device(backend, G: DeviceMatrix, N: int, k: int, U: DeviceMatrix,
-                          Rin: DeviceMatrix | None = None, Rout: DeviceMatrix | None = None):
+                          Rin: DeviceMatrix | None = None, Rout: DeviceMatrix | None = None,
+                          forced_unit_roundoff: float | None = None):
     """cholesky_upper(G, N, k) (src/panelblas.jl:148-155) on the device. Writes
     U; with Rin, also Rout = U Rin. Returns (shifted, shift). Waits for the
-    queue, since the caller branches on `shifted`."""
+    queue, since the caller branches on `shifted`. With forced_unit_roundoff
+    = u it factors G + s I at once, s = 11 (N k + k (k+1)) u ||G||_F: the
+    first pass of the shifted CholeskyQR3."""
     _need_complex128(G, U)
     if G.shape != (k, k) or U.shape != (k, k):
         raise DimensionMismatch(f"cholesky_upper: a {k}x{k} factor of a {G.shape} matrix into {U.shape}")
@@ -137,12 +140,18 @@ def cholesky_upper_device(backend, G: DeviceMatrix, N: int, k: int, U: DeviceMat
     shifted = ctypes.c_int(0)
     shift = ctypes.c_double(0.0)
     lib = _lib.load()
+    rin = (_vp(Rin.ptr if Rin is not None else None), Rin.ld if Rin is not None else k)
+    rout = (_vp(Rout.ptr if Rout is not None else None), Rout.ld if Rout is not None else k)
     try:
-        status = lib.fb_zpotrf_shifted(
-            _vp(U.ptr), U.ld, _vp(G.ptr), G.ld, k, N,
-            _vp(Rin.ptr if Rin is not None else None), Rin.ld if Rin is not None else k,
-            _vp(Rout.ptr if Rout is not None else None), Rout.ld if Rout is not None else k,
-            ctypes.byref(shifted), ctypes.byref(shift), _vp(ws), ws_bytes, backend.queue_handle())
+        if forced_unit_roundoff is None:
+            status = lib.fb_zpotrf_shifted(_vp(U.ptr), U.ld, _vp(G.ptr), G.ld, k, N, *rin, *rout,
+                                           ctypes.byref(shifted), ctypes.byref(shift), _vp(ws), ws_bytes,
+                                           backend.queue_handle())
+        else:
+            shifted.value = 1
+            status = lib.fb_zpotrf_forced_shift(_vp(U.ptr), U.ld, _vp(G.ptr), G.ld, k, N, *rin, *rout,
+                                                float(forced_unit_roundoff), ctypes.byref(shift), _vp(ws),
+                                                ws_bytes, backend.queue_handle())
     finally:
         backend.workspace_release()
     if status == _lib.FB_ENOTSPD:
@@ -158,14 +167,20 @@ def cholqr2_workspace_bytes(N: int, k: int) -> int:
     return need.value
 
 
-def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True, form: str = "fp64"):
+UNIT_ROUNDOFF = {np.dtype(np.complex128): 2.0 ** -53, np.dtype(np.complex64): 2.0 ** -24}
+
+
+def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = True, form: str = "fp64",
+                     unit_roundoff: float = UNIT_ROUNDOFF[np.dtype(np.complex128)]):
     """cholqr2! (src/panelblas.jl:130-139) on a matrix already in device
     memory: Y becomes Q in place and R (k x k) is written. With wait=True the
     call returns (passes, shifts) and raises if a Gram matrix stayed
     indefinite; with wait=False it only enqueues. form="tc" computes the Gram
-    matrices on the integer tensor cores (k <= 64)."""
-    if form not in ("fp64", "tc"):
-        raise ArgumentError(f"cholqr2! form is 'fp64' or 'tc', got {form!r}")
+    matrices on the integer tensor cores (k <= 64); form="shifted3" is the
+    shifted CholeskyQR3 (pass 1 shifted by 11 (N k + k (k+1)) u ||G||_F with
+    u = unit_roundoff, three passes)."""
+    if form not in ("fp64", "tc", "shifted3"):
+        raise ArgumentError(f"cholqr2! form is 'fp64', 'tc' or 'shifted3', got {form!r}")
     _need_complex128(Y, R)
     N, k = Y.shape
     if R.shape != (k, k):
@@ -177,10 +192,13 @@ def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = Tru
     info = ctypes.c_int(0)
     passes = ctypes.c_int(0)
     try:
-        entry = lib.fb_zcholqr2_tc if form == "tc" else lib.fb_zcholqr2
-        status = entry(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld,
-                                 ctypes.byref(info) if wait else None, ctypes.byref(passes) if wait else None,
-                                 _vp(ws), ws_bytes, backend.queue_handle())
+        out = (ctypes.byref(info) if wait else None, ctypes.byref(passes) if wait else None,
+               _vp(ws), ws_bytes, backend.queue_handle())
+        if form == "shifted3":
+            status = lib.fb_zcholqr3_shifted(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld, float(unit_roundoff), *out)
+        else:
+            entry = lib.fb_zcholqr2_tc if form == "tc" else lib.fb_zcholqr2
+            status = entry(_vp(Y.ptr), Y.ld, N, k, _vp(R.ptr), R.ld, *out)
     finally:
         backend.workspace_release()
     if not wait:

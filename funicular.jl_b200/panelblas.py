@@ -225,10 +225,12 @@ def panelmul(Y: PanelMatrix, G: DeviceOperator, X: PanelMatrix, *, nbuffers=None
 
 # ---- cholqr2! (src/panelblas.jl:130-169) --------------------------------------
 
-def cholesky_upper(plan, G_dev: DeviceMatrix, N: int, k: int, U_dev: DeviceMatrix):
+def cholesky_upper(plan, G_dev: DeviceMatrix, N: int, k: int, U_dev: DeviceMatrix, forced_unit_roundoff=None):
     """The device hook standing in for cholesky_upper (src/panelblas.jl:148-155):
-    returns shifted, with U_dev holding the factor."""
-    shifted, _ = kernels.cholesky_upper_device(plan.backend, G_dev, N, k, U_dev)
+    returns shifted, with U_dev holding the factor. forced_unit_roundoff
+    shifts at once (the first pass of the shifted CholeskyQR3)."""
+    shifted, _ = kernels.cholesky_upper_device(plan.backend, G_dev, N, k, U_dev,
+                                               forced_unit_roundoff=forced_unit_roundoff)
     return shifted
 
 
@@ -240,26 +242,28 @@ def rdiv_rows(Y: PanelMatrix, R_dev: DeviceMatrix, *, nbuffers=None) -> PanelMat
     return Y
 
 
-def cholqr_pass(Y: PanelMatrix, nbuffers, U_dev: DeviceMatrix, G_dev: DeviceMatrix):
+def cholqr_pass(Y: PanelMatrix, nbuffers, U_dev: DeviceMatrix, G_dev: DeviceMatrix, forced_unit_roundoff=None):
     """cholqr_pass! (src/panelblas.jl:141-146): one pass streamed through row
     sweeps, the k x k factor staying on the device."""
     plan = Y.plan
     backend = plan.backend
     sweep(lambda step, Yb: kernels.gram_accumulate(backend, G_dev, Yb, Yb, 1.0, carry(step)),
           readpanels(Y), nbuffers=nbuffers, traversal=rowtraversal(Y))
-    shifted = cholesky_upper(plan, G_dev, Y.N, Y.k, U_dev)
+    shifted = cholesky_upper(plan, G_dev, Y.N, Y.k, U_dev, forced_unit_roundoff)
     rdiv_rows(Y, U_dev, nbuffers=nbuffers)
     return collect_small(U_dev, plan), shifted
 
 
-def cholqr2_streamed(Y: PanelMatrix, *, nbuffers=None) -> np.ndarray:
+def cholqr2_streamed(Y: PanelMatrix, *, nbuffers=None, forced_unit_roundoff=None) -> np.ndarray:
     """cholqr2! as the reference runs it (src/panelblas.jl:130-139): two
-    passes, a third when either shifted, every pass two row sweeps."""
+    passes, a third when either shifted, every pass two row sweeps. With
+    forced_unit_roundoff the first pass is shifted at once, so all three run:
+    the shifted CholeskyQR3."""
     Y.assert_writable()
     plan = Y.plan
     G_dev, U_dev = checkout_device_buffers(plan, Y.dtype, (Y.k, Y.k), 2)
     try:
-        R, s1 = cholqr_pass(Y, nbuffers, U_dev, G_dev)
+        R, s1 = cholqr_pass(Y, nbuffers, U_dev, G_dev, forced_unit_roundoff)
         R2, s2 = cholqr_pass(Y, nbuffers, U_dev, G_dev)
         R = R2 @ R
         if s1 or s2:
@@ -278,7 +282,7 @@ def fits_on_device(Y: PanelMatrix) -> bool:
     return pool.allocated + need <= pool.budget
 
 
-def cholqr2_resident(Y: PanelMatrix) -> np.ndarray:
+def cholqr2_resident(Y: PanelMatrix, form: str = "fp64", unit_roundoff=None) -> np.ndarray:
     """The backend's cholqr2! when Y fits on the device: every panel goes up
     once, the whole two- or three-pass chain runs on the device
     (kernels.cholqr2_resident), Q comes back down once. Two host-device
@@ -296,7 +300,8 @@ def cholqr2_resident(Y: PanelMatrix) -> np.ndarray:
                 backend.wait_event(q, p.hold)
         to_device(Y, D, q)
         # Waits for the chain and raises NotPositiveDefinite if it stopped.
-        backend.submit(q, lambda: kernels.cholqr2_resident(backend, D, Rd, wait=True))
+        extra = {} if unit_roundoff is None else {"unit_roundoff": unit_roundoff}
+        backend.submit(q, lambda: kernels.cholqr2_resident(backend, D, Rd, wait=True, form=form, **extra))
         from_device(Y, D, q)
         R = np.empty((Y.k, Y.k), dtype=Y.dtype, order="F")
         backend.d2h(R, Rd, queue=q)
@@ -319,6 +324,31 @@ def cholqr2(Y: PanelMatrix, *, nbuffers=None, resident=None) -> np.ndarray:
     if resident:
         return cholqr2_resident(Y)
     return cholqr2_streamed(Y, nbuffers=nbuffers)
+
+
+def storage_unit_roundoff(Y: PanelMatrix) -> float:
+    """The unit roundoff of what Y holds between passes: its host storage
+    eltype's (ComplexF32 for a narrowed tier), else the compute eltype's."""
+    from .panels import host_storage_eltype
+    S = host_storage_eltype(Y.plan, Y.dtype)
+    return kernels.UNIT_ROUNDOFF.get(np.dtype(S), kernels.UNIT_ROUNDOFF[np.dtype(np.complex128)])
+
+
+def cholqr3(Y: PanelMatrix, *, nbuffers=None, resident=None, unit_roundoff=None) -> np.ndarray:
+    """The shifted CholeskyQR3 (Fukaya et al., SIAM J. Sci. Comput. 2020), the
+    north-star addition for the ComplexF32 storage tier: Y becomes Q in place
+    and R = R3 R2 R1 comes back. Pass 1 factors G + s I with
+    s = 11 (N k + k (k+1)) u ||G||_F whatever G's definiteness, passes 2 and
+    3 are plain. u defaults to the unit roundoff of Y's storage (2^-24 for a
+    ComplexF32 host tier, 2^-53 otherwise). Device-resident when Y fits,
+    streamed through row sweeps otherwise, like cholqr2."""
+    Y.assert_writable()
+    u = storage_unit_roundoff(Y) if unit_roundoff is None else float(unit_roundoff)
+    if resident is None:
+        resident = fits_on_device(Y)
+    if resident:
+        return cholqr2_resident(Y, form="shifted3", unit_roundoff=u)
+    return cholqr2_streamed(Y, nbuffers=nbuffers, forced_unit_roundoff=u)
 
 
 # ---- project (src/panelblas.jl:268-301) ---------------------------------------

@@ -219,6 +219,28 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
                       double* shifts /* 3 entries, or NULL */);
 
+/* The shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Zhang, Yamamoto,
+ * SIAM J. Sci. Comput. 2020), the orthonormalization the north-star backend
+ * adds for a ComplexF32 storage tier (no counterpart in the reference, whose
+ * cholqr2! shifts only a pass whose factorization failed,
+ * src/panelblas.jl:148-155): pass 1 factors G + s I unconditionally with
+ * s = 11 (N k + k (k+1)) u ||G||_F, passes 2 and 3 are plain, R = R3 R2 R1.
+ * unit_roundoff = u, in (0, 1): 2^-53 when Y holds FP64 values throughout,
+ * 2^-24 when it is rounded to ComplexF32 between passes. Same workspace,
+ * status and query as fb_zcholqr2; *passes = 3 on success. */
+int fb_zcholqr3_shifted(fb_z128* Y, int64_t ldy, int64_t N, int k,
+                        fb_z128* R, int64_t ldr, double unit_roundoff, int* info, int* passes,
+                        void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
+/* The first factorization of the shifted CholeskyQR3 for a caller that runs
+ * the passes itself (the streamed form): as fb_zpotrf_shifted, but G + s I is
+ * factored at once with s = 11 (N k + k (k+1)) u ||G||_F and not retried;
+ * *shift = s. Synchronizes `queue`; FB_ENOTSPD when even G + s I fails. */
+int fb_zpotrf_forced_shift(fb_z128* U, int64_t ldu, const fb_z128* G, int64_t ldg,
+                           int k, int64_t N, const fb_z128* Rin, int64_t ldrin,
+                           fb_z128* Rout, int64_t ldrout, double unit_roundoff, double* shift,
+                           void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
 /* ---- operators: src/operator.jl ------------------------------------- */
 
 /* The matrix-free operator of the streamed range finder: Y[:, c] <-

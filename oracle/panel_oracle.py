@@ -211,6 +211,32 @@ def cholqr2(Y, w=None):
     return R, passes
 
 
+def cholqr3_shifted(Y, u, w=None, storage=None):
+    """The shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Zhang, Yamamoto,
+    SIAM J. Sci. Comput. 2020) the north-star backend adds; not in the
+    reference. Pass 1 factors G + s I with s = 11 (N k + k (k+1)) u ||G||_F
+    unconditionally, passes 2 and 3 are cholqr_pass (src/panelblas.jl:141-146),
+    R = R3 R2 R1. With storage (a numpy dtype) Y is rounded to it after every
+    pass, as a narrowed host tier holds it between passes. Returns R."""
+    N, k = Y.shape
+    G = gram(Y, w=w)
+    shift = 11 * (N * k + k * (k + 1)) * u * np.linalg.norm(G)
+    potrf = lapack.zpotrf if np.iscomplexobj(G) else lapack.dpotrf
+    R, info = potrf(np.asfortranarray(G + shift * np.eye(k)), lower=0, clean=1)
+    if info != 0:
+        raise OracleArgumentError(f"the {k}x{k} Gram matrix is not positive definite even after a shift of {shift}")
+    R = np.triu(R)
+    rdiv_rows(Y, R, w)
+    if storage is not None:
+        Y[...] = Y.astype(storage)
+    for _ in range(2):
+        R2, _ = cholqr_pass(Y, w)
+        if storage is not None:
+            Y[...] = Y.astype(storage)
+        R = R2 @ R
+    return R
+
+
 def panelmul(G, X, w=None):
     """panelmul!(Y, G, X) (src/panelblas.jl:91-100): Y[:, panel] = G X[:, panel]."""
     k = X.shape[1]

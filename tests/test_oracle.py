@@ -128,3 +128,30 @@ def test_kernels_against_dense(oracle):
     Z = Y.copy(order="F")
     oracle.rdiv_upper(Z, R)
     np.testing.assert_allclose(Z, Y @ np.linalg.inv(R), rtol=oracle.blastol(np.complex128, 7, 5))
+
+
+# ---- the shifted CholeskyQR3 (the ComplexF32 storage tier's orthonormalization)
+
+@pytest.mark.parametrize("kappa", [1e4, 1e7, 1e12])
+def test_cholqr3_shifted_orthonormalizes_past_cholqr2_range(oracle, kappa):
+    # The shift makes pass 1 succeed for condition numbers far past what the
+    # unshifted CholeskyQR2 handles (about 1e8 in FP64).
+    from conftest import conditioned
+    rng = np.random.default_rng(int(np.log10(kappa)))
+    A = conditioned(rng, 3000, 24, kappa)
+    Q = A.copy(order="F")
+    R = oracle.cholqr3_shifted(Q, 2.0 ** -53)
+    assert oracle.orthogonality_error(Q) < 1e-13
+    assert oracle.reconstruction_error(A, Q, R) < 1e-14
+    assert np.allclose(np.tril(R, -1), 0)
+
+
+def test_cholqr3_shifted_with_complex64_storage(oracle):
+    from conftest import conditioned
+    rng = np.random.default_rng(5)
+    A = conditioned(rng, 4000, 16, 1e5).astype(np.complex64).astype(np.complex128)
+    Q = A.copy(order="F")
+    R = oracle.cholqr3_shifted(Q, 2.0 ** -24, storage=np.complex64)
+    assert np.array_equal(Q, Q.astype(np.complex64).astype(np.complex128))
+    assert oracle.orthogonality_error(Q) < 1e-5
+    assert oracle.reconstruction_error(A, Q, R) < 1e-6

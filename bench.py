@@ -59,6 +59,8 @@ def parse_args():
                    help="instances of the batched cholqr2! measurement (0 skips it)")
     p.add_argument("--wide-N", type=int, default=10_000_000,
                    help="rows of the k = 128 configuration (0 skips it)")
+    p.add_argument("--rf-k", type=int, default=24, help="columns of the streamed range finder (0 skips it)")
+    p.add_argument("--rf-budget-gib", type=int, default=12, help="device budget of the streamed range finder")
     p.add_argument("--adjoint-N", type=int, default=1 << 22,
                    help="rows of the differentiation workload (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace",
@@ -383,6 +385,95 @@ def run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, ba
                             "clock": "host wall clock around the synchronous call, 2 calls after one warm-up"})
         fb.free(Ypm)
         del Ypm, plan
+    return out
+
+
+def measure_pcie(torch, device):
+    """Page-locked copy bandwidth of this box, best of a few 1 GiB copies each
+    way (cudaMemcpyAsync through torch): the streamed path's roofline."""
+    n = 1 << 30
+    h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(n, dtype=torch.uint8, device=device)
+    out = {}
+    for name, fn in (("h2d", lambda: d.copy_(h, non_blocking=True)), ("d2h", lambda: h.copy_(d, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms = a.elapsed_time(b)
+            best = ms if best is None else min(best, ms)
+        out[name] = n / (best * 1e-3) / 1e9
+    del h, d
+    return out
+
+
+def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, barrier):
+    """The streamed range finder (config C4, scaled): G = -Lap_7 + (0.5+0.1i) I
+    on the 342^3 grid (N = 40 001 688) applied matrix-free, X = GhostPanels
+    (filled on the device), Y = panelmul(G, X), cholqr2 of Y through row
+    sweeps, S = project(Y, G), with the plan's device budget below the matrix
+    so every panel streams through page-locked host memory. k = args.rf_k and
+    the budget are scaled down from 256 and 40 GB so one step fits the bench:
+    project moves p (p + 1) panels, quadratic in the panel count. Each phase is
+    timed on the host clock around its synchronous call; the bytes that cross
+    the bus are counted from the panel widths and set against the measured
+    page-locked copy bandwidth."""
+    grid = (342, 342, 342)
+    N = grid[0] * grid[1] * grid[2]
+    k = args.rf_k
+    # Host blocks are whole panels of the plan's width (the last one too).
+    plan = fb.ResidencyPlan(device_budget=args.rf_budget_gib * fb.GiB, host_budget=int(1.5 * N * k * 16) + 4 * fb.GiB,
+                            backend=backend)
+    X = fb.GhostPanels(np.complex128, N, k, plan=plan, seed=0xC4)
+    Y = fb.PanelMatrix.undef(np.complex128, N, k, plan=plan, w=X.w)
+    G = fb.Laplacian7(grid, 0.5 + 0.1j)
+    pcie = measure_pcie(torch, device)
+
+    def step():
+        t = [time.perf_counter()]
+        fb.panelmul(Y, G, X)
+        t.append(time.perf_counter())
+        R = fb.cholqr2(Y, resident=False)
+        t.append(time.perf_counter())
+        S = fb.project(Y, G)
+        t.append(time.perf_counter())
+        return [1e3 * (t[i + 1] - t[i]) for i in range(3)], R, S
+
+    barrier()
+    step()
+    barrier()
+    ms, R, S = step()
+    ms = [max_over_ranks(x) for x in ms]
+    widths = [Y.panelwidth(j) for j in range(Y.npanels())]
+    p = len(widths)
+    col = 16 * N
+    passes = 2  # the third pass runs only after a shift, and the Gram of G X is well conditioned here
+    # Host to device and back, per phase: panelmul writes Y (X is generated on
+    # the device); a cholqr2 pass reads Y twice (Gram, solve) and writes it
+    # once; project uploads p (p + 1) panels.
+    up = {"panelmul": 0, "cholqr2": passes * 2 * col * k, "project": col * sum(widths) + col * p * sum(widths)}
+    down = {"panelmul": col * k, "cholqr2": passes * col * k, "project": 0}
+    Gq = fb.gram(Y)
+    orth = float(np.linalg.norm(Gq - np.eye(k)))
+    total_ms = sum(ms)
+    total_bus = sum(up.values()) + sum(down.values())
+    # The link carries both directions at once: the bound is the slower
+    # direction's bytes over its measured bandwidth.
+    bound_ms = 1e3 * max(sum(up.values()) / (pcie["h2d"] * 1e9), sum(down.values()) / (pcie["d2h"] * 1e9))
+    out = {"workload": f"streamed range finder, 342^3 Laplacian (N={N}), k={k}, {p} panels of width {max(widths)}, "
+                       f"device budget {args.rf_budget_gib} GiB for a {col * k / 1e9:.1f} GB matrix",
+           "ms": {"panelmul": ms[0], "cholqr2_streamed": ms[1], "project": ms[2], "step": total_ms},
+           "bus_bytes_up": up, "bus_bytes_down": down, "bus_gbs": total_bus / (total_ms * 1e-3) / 1e9,
+           "pcie_measured_gbs": pcie, "ms_pcie_bound": bound_ms, "pcie_roofline_frac": bound_ms / total_ms,
+           "orthogonality_fro": orth, "r_finite": bool(np.isfinite(R).all()), "s_finite": bool(np.isfinite(S).all()),
+           "clock": "host wall clock around each synchronous call, the second of two steps"}
+    fb.free(Y)
+    del X, Y, plan
     return out
 
 
@@ -760,6 +851,8 @@ def run_ours(args):
             if args.wide_N > 0 else None)
     if wide is not None and args.e2e_steps > 0:
         wide["storage"] = run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, barrier)
+    range_finder = (run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, barrier)
+                    if args.rf_k > 0 else None)
     adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.adjoint_N > 0 else None)
     if adjoint is not None:
@@ -824,7 +917,7 @@ def run_ours(args):
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
                      "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
-        "tensor_form": tensor_form, "batched": batched, "wide": wide, "adjoint": adjoint,
+        "tensor_form": tensor_form, "batched": batched, "wide": wide, "range_finder": range_finder, "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

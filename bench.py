@@ -282,7 +282,7 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
             "alg_bytes_per_step": alg, "ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
             "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
             "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,
-            "launch": "one fb_zcholqr2_batched call, replayed as one captured CUDA graph"}
+            "launch": "one fb_zcholqr2_batched call (eight stream lanes), replayed as one captured CUDA graph"}
 
 
 def run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak):

@@ -10,6 +10,10 @@
 // later kernel (Y keeps what the finished passes made of it, as when the
 // reference throws before its rdiv_rows!), and the third pass runs only if a
 // shift fired in pass 1 or 2.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
 #include "fb_common.cuh"
 
 namespace fb {
@@ -145,10 +149,34 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
     return FB_OK;
 }
 
-// A batch: one status block per instance, then one scratch area sized for
-// the largest instance, reused by every instance in turn (they run one after
-// another on the queue).
+// A batch runs on up to BATCH_LANES library-owned streams ("lanes") forked
+// from the caller's queue and joined back into it with events, so the
+// one-CTA kernels of one instance (the Cholesky, the solve's prep) run beside
+// the full-GPU kernels of others instead of leaving the GPU idle. Each
+// instance's chain is the same launch sequence as a single call, on one lane:
+// its bits do not depend on the batch. The workspace holds one status block
+// per instance, then one scratch area per lane sized for the largest
+// instance. Fork and join are plain event records and waits, so a captured
+// batch is one graph with the lanes as parallel branches.
+constexpr int BATCH_LANES = 8;
 static size_t batch_status_bytes(int count) { return align_up((size_t)count * sizeof(ChainStatus), 256); }
+static int batch_lanes(int count) { return count < BATCH_LANES ? count : BATCH_LANES; }
+
+// The lane streams of the current device, created once.
+static int lane_streams(cudaStream_t* out, int n) {
+    static std::mutex mu;
+    static cudaStream_t lanes[64][BATCH_LANES] = {};
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) { set_error(FB_ENOTSUP, "cholqr2! batch: device %d", dev); return FB_ENOTSUP; }
+    std::lock_guard<std::mutex> lock(mu);
+    for (int l = 0; l < n; ++l) {
+        if (!lanes[dev][l])
+            FB_CUDA(cudaStreamCreateWithFlags(&lanes[dev][l], cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+        out[l] = lanes[dev][l];
+    }
+    return FB_OK;
+}
 
 int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr, int* info, int* passes,
                 void* workspace, size_t workspace_bytes, fb_queue_t queue) {
@@ -188,7 +216,7 @@ int fb_zcholqr2_batched_workspace_size(const int64_t* N, const int* k, int count
         const size_t t = cholqr_layout(N[i], k[i]).total;
         if (t > scratch) scratch = t;
     }
-    *bytes = batch_status_bytes(count) + scratch;
+    *bytes = batch_status_bytes(count) + (size_t)batch_lanes(count) * align_up(scratch, 256);
     return FB_OK;
 }
 
@@ -207,18 +235,64 @@ int fb_zcholqr2_batched(fb_z128* const* Y, const int64_t* ldy, const int64_t* N,
                   need, workspace_bytes);
         return FB_ENOMEM;
     }
-    ChainStatus* status = static_cast<ChainStatus*>(workspace);
-    char* scratch = static_cast<char*>(workspace) + batch_status_bytes(count);
-    const size_t scratch_bytes = workspace_bytes - batch_status_bytes(count);
-    for (int i = 0; i < count; ++i) {
+    for (int i = 0; i < count; ++i)
         if (tensor_form && k[i] > 64) {
             set_error(FB_ENOTSUP, "cholqr2! batch: the tensor-core form handles k <= 64, instance %d has k=%d", i, k[i]);
             return FB_ENOTSUP;
         }
-        FB_TRY(cholqr2_chain(Y[i], ldy[i], N[i], k[i], R[i], ldr[i], nullptr, nullptr, scratch, scratch_bytes, queue,
-                             tensor_form != 0, status + i));
+    ChainStatus* status = static_cast<ChainStatus*>(workspace);
+    const int L = batch_lanes(count);
+    const size_t lane_bytes = (workspace_bytes - batch_status_bytes(count)) / L / 256 * 256;
+    char* scratch = static_cast<char*>(workspace) + batch_status_bytes(count);
+    cudaStream_t lanes[BATCH_LANES];
+    FB_TRY(lane_streams(lanes, L));
+    // Longest first, each to the lane with the least work so far (work ~ N k^2).
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (double)N[a] * k[a] * k[a] > (double)N[b] * k[b] * k[b];
+    });
+    std::vector<double> load(L, 0.0);
+    std::vector<int> lane_of(count);
+    for (int i : order) {
+        int best = 0;
+        for (int l = 1; l < L; ++l)
+            if (load[l] < load[best]) best = l;
+        lane_of[i] = best;
+        load[best] += (double)N[i] * k[i] * k[i];
     }
-    return FB_OK;
+    cudaStream_t origin = stream_of(queue);
+    cudaEvent_t fork = nullptr, join[BATCH_LANES] = {};
+    auto release = [&]() {
+        if (fork) cudaEventDestroy(fork);
+        for (int l = 0; l < L; ++l)
+            if (join[l]) cudaEventDestroy(join[l]);
+    };
+    auto cu = [](cudaError_t err, const char* what) { return err == cudaSuccess ? FB_OK : cuda_status(err, what); };
+    int rc = FB_OK;
+    do {
+        if ((rc = cu(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreateWithFlags")))
+            break;
+        if ((rc = cu(cudaEventRecord(fork, origin), "cudaEventRecord"))) break;
+        for (int l = 0; l < L && !rc; ++l)
+            rc = cu(cudaStreamWaitEvent(lanes[l], fork, 0), "cudaStreamWaitEvent");
+        for (int i : order) {
+            if (rc) break;
+            const int l = lane_of[i];
+            rc = cholqr2_chain(Y[i], ldy[i], N[i], k[i], R[i], ldr[i], nullptr, nullptr, scratch + l * lane_bytes,
+                               lane_bytes, reinterpret_cast<fb_queue_t>(lanes[l]), tensor_form != 0, status + i);
+        }
+        // Join every lane back into the caller's queue, also after a failure,
+        // so nothing the lanes hold outlives the call unordered.
+        for (int l = 0; l < L; ++l) {
+            int j = cu(cudaEventCreateWithFlags(&join[l], cudaEventDisableTiming), "cudaEventCreateWithFlags");
+            if (!j) j = cu(cudaEventRecord(join[l], lanes[l]), "cudaEventRecord");
+            if (!j) j = cu(cudaStreamWaitEvent(origin, join[l], 0), "cudaStreamWaitEvent");
+            if (!rc) rc = j;
+        }
+    } while (false);
+    release();
+    return rc;
 }
 
 int fb_zcholqr2_batched_query(const void* workspace, int count, int* info, int* passes) {

@@ -281,8 +281,10 @@ int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k,
 /* Many independent cholqr2! instances of uneven N and k (the batched range
  * finder; no counterpart in the reference, which orthonormalizes one
  * PanelMatrix per call): instance i is Y[i] (N[i] x k[i], leading dimension
- * ldy[i]) with its R in R[i] (ldr[i]). The instances' chains are enqueued one
- * after another on `queue` and share one scratch area; each keeps its own
+ * ldy[i]) with its R in R[i] (ldr[i]). The instances' chains run on up to
+ * eight library-owned streams forked from `queue` and joined back into it
+ * (each chain on one stream, in the same launch sequence as a single call,
+ * so each instance's bits equal its own fb_zcholqr2's); each keeps its own
  * status block, read by fb_zcholqr2_batched_query after the queue drained
  * (info[i] = the failing pass or 0, passes[i] = 2 or 3). tensor_form != 0
  * runs every Gram on the integer tensor cores (all k[i] <= 64). Nothing

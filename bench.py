@@ -277,8 +277,29 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
     ms_eager = timed(eager)
     ms_graph = timed(lambda: graph.launch(queue))
     alg = float(sum(96.0 * N * k for N, k in zip(Ns, ks)))
-    del graph, tensors, Ys
+    del graph
+    # The same batch after the autotuner has chosen the Gram's row chunks for
+    # each shape class of the batch (each class tuned at its largest N).
+    shapes = [(int(N), int(k)) for N, k in zip(Ns, ks)]
+    t0 = time.perf_counter()
+    tuned = fb.autotune.tune_shapes(backend, shapes, forms=False)
+    lanes = fb.autotune.tune_batch_lanes(backend, Ys, Rs)
+    tune_s = time.perf_counter() - t0
+    nbytes_t = fb.kernels.cholqr2_batched_workspace_bytes(shapes)
+    ws_buf_t = backend.alloc_device(np.complex128, (nbytes_t // 16 + 32, 1))
+    ws_t = ((ws_buf_t.ptr + 255) // 256 * 256, nbytes_t)
+    graph_t = backend.capture(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws_t))
+    ms_tuned = timed(lambda: graph_t.launch(queue))
+    passes_t = []
+    backend.submit(queue, lambda: passes_t.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws_t)))
+    shifts = sorted({r["gram_shift"] for r in tuned})
+    fb.autotune.clear()
+    del graph_t, tensors, Ys
     return {"instances": count, "N_range": [int(Ns.min()), int(Ns.max())], "k_values": [16, 32, 64],
+            "tuned": {"ms_per_step_graph": ms_tuned, "value_graph": whole_job_gbs(alg, world, ms_tuned),
+                      "shape_classes": len(tuned), "gram_shifts_chosen": shifts, "lanes": lanes["lanes"],
+                      "ms_by_lanes_eager": lanes["ms"], "tuning_s": tune_s,
+                      "passes_max": max(passes_t)},
             "alg_bytes_per_step": alg, "ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
             "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
             "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,

@@ -23,6 +23,7 @@ from .panelblas import (gram, panelmul, cholqr2, cholqr3, project, rightmul, Den
 from .ghosts import GhostPanels, isghost
 from . import autodiff
 from .autodiff import rrule
+from . import autotune
 
 __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceError",
            "OutOfDeviceMemory", "B200Backend", "DeviceMatrix", "HostSlab", "b200_backend",
@@ -31,4 +32,4 @@ __all__ = ["ArgumentError", "DimensionMismatch", "NotPositiveDefinite", "DeviceE
            "PanelMatrix", "free", "sweep", "foreachpanel", "readpanels", "writepanels", "updatepanels",
            "PanelSteps", "RowSteps", "rowtraversal", "gram", "panelmul", "cholqr2", "cholqr3", "project", "rightmul",
            "DenseOperator", "ColumnOperator", "DeviceOperator", "Laplacian7", "HermitianBand", "cholesky_upper", "GhostPanels", "isghost",
-           "autodiff", "rrule"]
+           "autodiff", "rrule", "autotune"]

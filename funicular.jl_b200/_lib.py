@@ -121,6 +121,11 @@ SIGNATURES = {
     "fb_zproject_adjoint_workspace_size": [_int, _psz],
     "fb_zproject_adjoint": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, _vp, _sz, _vp],
     "fb_zhband_apply": [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _int, _vp],
+    "fb_tune_set_gram_chunks": [_i64, _int, _int],
+    "fb_tune_get_gram_chunks": [_i64, _int, _pint],
+    "fb_tune_clear": [],
+    "fb_tune_set_batch_lanes": [_int],
+    "fb_tune_get_batch_lanes": [_pint],
     "fb_zcholqr3_shifted": [_vp, _i64, _i64, _int, _vp, _i64, ctypes.c_double, _pint, _pint, _vp, _sz, _vp],
     "fb_zpotrf_forced_shift": [_vp, _i64, _vp, _i64, _int, _i64, _vp, _i64, _vp, _i64, ctypes.c_double, _pdbl,
                                _vp, _sz, _vp],

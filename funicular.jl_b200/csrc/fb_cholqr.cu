@@ -11,6 +11,7 @@
 // reference throws before its rdiv_rows!), and the third pass runs only if a
 // shift fired in pass 1 or 2.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -149,7 +150,7 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
     return FB_OK;
 }
 
-// A batch runs on up to BATCH_LANES library-owned streams ("lanes") forked
+// A batch runs on up to 8 (tunable to 1..16) library-owned streams ("lanes") forked
 // from the caller's queue and joined back into it with events, so the
 // one-CTA kernels of one instance (the Cholesky, the solve's prep) run beside
 // the full-GPU kernels of others instead of leaving the GPU idle. Each
@@ -158,9 +159,13 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
 // per instance, then one scratch area per lane sized for the largest
 // instance. Fork and join are plain event records and waits, so a captured
 // batch is one graph with the lanes as parallel branches.
-constexpr int BATCH_LANES = 8;
+constexpr int BATCH_LANES = 16;        // most lanes a batch can use
+static std::atomic<int> g_batch_lanes{8};  // lanes a batch uses: the autotuner's entry, 8 untuned
 static size_t batch_status_bytes(int count) { return align_up((size_t)count * sizeof(ChainStatus), 256); }
-static int batch_lanes(int count) { return count < BATCH_LANES ? count : BATCH_LANES; }
+static int batch_lanes(int count) {
+    const int lanes = g_batch_lanes.load();
+    return count < lanes ? count : lanes;
+}
 
 // The lane streams of the current device, created once.
 static int lane_streams(cudaStream_t* out, int n) {
@@ -330,6 +335,21 @@ int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shi
                   host.failed, host.shift[host.failed]);
         return FB_ENOTSPD;
     }
+    return FB_OK;
+}
+
+int fb_tune_set_batch_lanes(int lanes) {
+    if (lanes < 1 || lanes > BATCH_LANES) {
+        set_error(FB_EINVAL, "fb_tune_set_batch_lanes: lanes must lie in [1, %d], got %d", BATCH_LANES, lanes);
+        return FB_EINVAL;
+    }
+    g_batch_lanes.store(lanes);
+    return FB_OK;
+}
+
+int fb_tune_get_batch_lanes(int* lanes) {
+    if (!lanes) { set_error(FB_EINVAL, "fb_tune_get_batch_lanes: NULL"); return FB_EINVAL; }
+    *lanes = g_batch_lanes.load();
     return FB_OK;
 }
 

@@ -29,6 +29,7 @@
 // and 128-byte swizzling stores the 16-byte element of row r in column c at
 // chunk r ^ (c % 8) of that column's 128-byte line. The eight lanes that read
 // eight consecutive columns of one row therefore hit eight different banks.
+#include <map>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -344,6 +345,26 @@ __global__ void gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int kA, int
     *dst = out;
 }
 
+// The autotuner's table: for a shape class (floor(log2 rows), max(kA, kB)), a
+// shift of the row-chunk count. 0 (untuned) is one wave of CTAs; s > 0
+// divides the chunk count by 2^s (longer chunks, fewer partial tiles),
+// s < 0 multiplies it (shorter chunks, more CTAs). The chunk count sets the
+// order of the reduction, so a shape's bits follow its table entry.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, int>, int> g_tune_gram;
+
+static int shape_class(int64_t rows) {
+    int c = 0;
+    while (c < 62 && ((int64_t)1 << (c + 1)) <= rows) ++c;
+    return c;
+}
+
+static int tuned_gram_shift(int64_t rows, int kA, int kB) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_gram.find({shape_class(rows), kA > kB ? kA : kB});
+    return it == g_tune_gram.end() ? 0 : it->second;
+}
+
 static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian, int ctas_per_sm) {
     GramShape sh{};
     auto tile_width = [](int k) { int w = k < G_TILE ? k : G_TILE; return (w + 7) / 8 * 8; };
@@ -365,6 +386,9 @@ static GramShape gram_shape(int64_t rows, int kA, int kB, int hermitian, int cta
     }
     const int64_t stages = (rows + GS_ROWS - 1) / GS_ROWS;
     int64_t target = (int64_t)sm_count() * ctas_per_sm / smallest_launch;
+    const int shift = tuned_gram_shift(rows, kA, kB);
+    if (shift > 0) target >>= shift;
+    else if (shift < 0) target <<= -shift;
     if (target < 1) target = 1;
     if (target > stages) target = stages;
     if (target < 1) target = 1;
@@ -634,6 +658,30 @@ int fb_zgram_static(fb_z128* C, int64_t ldc, const fb_z128* A, int64_t lda, cons
     return gram_enqueue(reinterpret_cast<z64*>(C), ldc, reinterpret_cast<const z64*>(A), lda,
                         reinterpret_cast<const z64*>(B), ldb, rows, kA, kB, a, b, hermitian,
                         scratch, GRAM_STATIC_SCRATCH_BYTES, stream_of(queue), nullptr, GATE_ALWAYS);
+}
+
+int fb_tune_set_gram_chunks(int64_t rows, int k, int shift) {
+    if (rows < 1 || k < 1 || shift < -3 || shift > 8) {
+        set_error(FB_EINVAL, "fb_tune_set_gram_chunks: rows %lld, k %d, shift %d (shift in [-3, 8])", (long long)rows, k,
+                  shift);
+        return FB_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (shift == 0) g_tune_gram.erase({shape_class(rows), k});
+    else g_tune_gram[{shape_class(rows), k}] = shift;
+    return FB_OK;
+}
+
+int fb_tune_get_gram_chunks(int64_t rows, int k, int* shift) {
+    if (rows < 1 || k < 1 || !shift) { set_error(FB_EINVAL, "fb_tune_get_gram_chunks: bad argument"); return FB_EINVAL; }
+    *shift = tuned_gram_shift(rows, k, k);
+    return FB_OK;
+}
+
+int fb_tune_clear(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_gram.clear();
+    return FB_OK;
 }
 
 }  // extern "C"

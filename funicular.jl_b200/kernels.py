@@ -178,11 +178,15 @@ def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = Tru
     indefinite; with wait=False it only enqueues. form="tc" computes the Gram
     matrices on the integer tensor cores (k <= 64); form="shifted3" is the
     shifted CholeskyQR3 (pass 1 shifted by 11 (N k + k (k+1)) u ||G||_F with
-    u = unit_roundoff, three passes)."""
-    if form not in ("fp64", "tc", "shifted3"):
-        raise ArgumentError(f"cholqr2! form is 'fp64', 'tc' or 'shifted3', got {form!r}")
+    u = unit_roundoff, three passes); form="auto" takes the form the
+    autotuner chose for this shape ("fp64" when untuned)."""
+    if form not in ("fp64", "tc", "shifted3", "auto"):
+        raise ArgumentError(f"cholqr2! form is 'fp64', 'tc', 'shifted3' or 'auto', got {form!r}")
     _need_complex128(Y, R)
     N, k = Y.shape
+    if form == "auto":
+        from . import autotune
+        form = autotune.form_for(N, k)
     if R.shape != (k, k):
         raise DimensionMismatch(f"cholqr2! of an {N}x{k} matrix writes a {k}x{k} R, got {R.shape}")
     need = ctypes.c_size_t(0)

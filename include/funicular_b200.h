@@ -282,7 +282,8 @@ int fb_zcholqr2_tc(fb_z128* Y, int64_t ldy, int64_t N, int k,
  * finder; no counterpart in the reference, which orthonormalizes one
  * PanelMatrix per call): instance i is Y[i] (N[i] x k[i], leading dimension
  * ldy[i]) with its R in R[i] (ldr[i]). The instances' chains run on up to
- * eight library-owned streams forked from `queue` and joined back into it
+ * eight (fb_tune_set_batch_lanes) library-owned streams forked from `queue`
+ * and joined back into it
  * (each chain on one stream, in the same launch sequence as a single call,
  * so each instance's bits equal its own fb_zcholqr2's); each keeps its own
  * status block, read by fb_zcholqr2_batched_query after the queue drained
@@ -342,6 +343,26 @@ int fb_zproject_adjoint(fb_z128* Qbar, int64_t ldqb, const fb_z128* GQ, int64_t 
 int fb_zhband_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx,
                     const fb_z128* Dg, int64_t lddg, int64_t N, int kd, int cols,
                     fb_queue_t queue);
+
+/* ---- autotuning -------------------------------------------------------
+ * No counterpart in the reference. The library keeps a table of tile-shape
+ * choices per shape class (floor(log2 rows), columns) that its kernels read
+ * when they lay out a launch; an autotuner (funicular_b200.autotune) times
+ * candidates on the device and fills it. Untuned shapes keep the built-in
+ * choice. For the Gram, the entry is a shift of its row-chunk count: 0 is
+ * one wave of CTAs over the GPU, s > 0 divides the count by 2^s (longer
+ * chunks), s < 0 multiplies it (shorter ones); shift in [-3, 8]. The chunk
+ * count fixes the reduction order, so a shape's results are reproducible to
+ * the bit for a fixed table, and fb_zgram_workspace_size follows the table:
+ * tune before sizing workspaces. */
+int fb_tune_set_gram_chunks(int64_t rows, int k, int shift);
+int fb_tune_get_gram_chunks(int64_t rows, int k, int* shift);
+/* Clears the Gram entries (the batch's lane count is kept). */
+int fb_tune_clear(void);
+/* The number of stream lanes fb_zcholqr2_batched spreads a batch over, in
+ * [1, 16], 8 untuned; fb_zcholqr2_batched_workspace_size follows it. */
+int fb_tune_set_batch_lanes(int lanes);
+int fb_tune_get_batch_lanes(int* lanes);
 
 /* ---- ghost panels: src/ghosts.jl ------------------------------------- */
 

@@ -109,3 +109,25 @@ def test_errors_are_per_thread(fb):
     t.join()
     assert seen == [""]
     assert fb._lib.last_error() != ""
+
+
+def test_tuning_table_is_host_state(fb, tmp_path):
+    # The autotuner's table lives in the library's host memory: it can be set,
+    # read, saved, loaded and cleared without a GPU.
+    fb.autotune.clear()
+    assert fb.autotune.gram_shift(10_000, 16) == 0
+    fb.autotune.set_gram_shift(10_000, 16, 2)
+    assert fb.autotune.gram_shift(16_383, 16) == 2      # same class: floor(log2 N) = 13
+    assert fb.autotune.gram_shift(16_384, 16) == 0      # next class
+    assert fb.autotune.gram_shift(10_000, 32) == 0
+    fb.autotune._records[(13, 16)] = {"N": 10_000, "k": 16, "class": 13, "gram_shift": 2, "form": "tc"}
+    fb.autotune._forms[(13, 16)] = "tc"
+    path = tmp_path / "tune.json"
+    fb.autotune.save(str(path))
+    fb.autotune.clear()
+    assert fb.autotune.gram_shift(10_000, 16) == 0 and fb.autotune.form_for(10_000, 16) == "fp64"
+    fb.autotune.load(str(path))
+    assert fb.autotune.gram_shift(10_000, 16) == 2 and fb.autotune.form_for(10_000, 16) == "tc"
+    with pytest.raises(fb.ArgumentError):
+        fb.autotune.set_gram_shift(10_000, 16, 9)
+    fb.autotune.clear()

@@ -29,14 +29,17 @@ class SweepOperand:
 
 
 def readpanels(pm):
+    """readpanels(pm) (src/executor.jl:9): a sweep operand staged up, not written back."""
     return SweepOperand(pm, True, False)
 
 
 def writepanels(pm):
+    """writepanels(pm) (src/executor.jl:10): a sweep operand written back, not staged up (its buffer starts undefined)."""
     return SweepOperand(pm, False, True)
 
 
 def updatepanels(pm):
+    """updatepanels(pm) (src/executor.jl:11): a sweep operand staged up and written back."""
     return SweepOperand(pm, True, True)
 
 
@@ -115,6 +118,7 @@ class RowSteps:
 
 
 def rowtraversal(pm: PanelMatrix) -> RowSteps:
+    """rowtraversal(pm) (src/executor.jl:38): row blocks of row_block_height rows."""
     return RowSteps(pm.N, row_block_height(pm.N, pm.k, pm.w))
 
 
@@ -244,16 +248,23 @@ def sweep(f, *operands: SweepOperand, nbuffers=None, traversal=None) -> None:
     finally:
         stop.set()
         producer.join()
-        for q in (up, compute, down):
-            try:
-                backend.sync_queue(q)
-            except Exception:
-                pass
+        sync_quietly(backend, (up, compute, down))
         for b in buffers:
             checkin_device_buffers(plan, b)
         for s in staging:
             if s is not None:
                 checkin_device_buffers(plan, s)
+
+
+def sync_quietly(backend, queues) -> None:
+    """sync_quietly (src/executor.jl:113-122): drains the queues on the way out
+    of a sweep, failed or not, so no pending copy still uses a staging buffer
+    once it goes back to the pool; a failure here was already raised."""
+    for q in queues:
+        try:
+            backend.sync_queue(q)
+        except Exception:
+            pass
 
 
 def foreachpanel(f, pm: PanelMatrix, *, write=True, nbuffers=None) -> None:

@@ -105,4 +105,5 @@ def GhostPanels(dtype, N: int, k: int, *, plan, seed=0, w=None, generator=None) 
 
 
 def isghost(pm: PanelMatrix) -> bool:
+    """Whether pm is a GhostPanels matrix (regenerated from its seed, never stored)."""
     return pm.is_ghost()

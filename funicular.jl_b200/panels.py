@@ -136,8 +136,7 @@ class PanelMatrix:
             self.ghost.collect_into(self, out)
             return out
         for j, p in enumerate(self.panels):
-            if p.hold is not None:
-                self.plan.backend.sync_event(p.hold)
+            wait_hold(self.plan, p)
             cols = self.panelrange(j)
             out[:, cols.start:cols.stop] = p.storage()
         return out
@@ -255,11 +254,19 @@ def from_device(pm: PanelMatrix, src: DeviceMatrix, queue=None):
     return event
 
 
+def wait_hold(plan, panel) -> None:
+    """Waits for whatever copy last read or wrote the panel's host memory
+    (its hold event), before the host reads the panel or gives its block
+    back: the wait of spill! (src/panels.jl:512-520)."""
+    if panel.hold is not None:
+        plan.backend.sync_event(panel.hold)
+        panel.hold = None
+
+
 def free(pm: PanelMatrix) -> None:
     """free! (src/panels.jl:540-555): gives every panel's host block back."""
     for p in pm.panels:
         if p.data is not None:
-            if p.hold is not None:
-                pm.plan.backend.sync_event(p.hold)
+            wait_hold(pm.plan, p)
             release_host_block(pm.plan, p.data.block)
             p.data = None

@@ -218,6 +218,8 @@ def checkin_device_buffers(plan: ResidencyPlan, buffers) -> None:
 
 
 def device_bytes_allocated(plan: ResidencyPlan) -> int:
+    """Bytes the plan's device pool holds (src/plan.jl:159-185): every buffer
+    it has checked out so far, in use or free, counted against device_budget."""
     return plan.devicepool.allocated
 
 
@@ -283,8 +285,12 @@ def host_bytes_reserved(pool) -> int:
 
 
 def host_bytes_free(pool) -> int:
+    """Bytes of given-back host blocks waiting in the pool for reuse
+    (src/plan.jl:322-334); takes the pool or its plan."""
     return sum(b.nbytes for blocks in _hostpool(pool).free.values() for b in blocks)
 
 
 def host_bytes_in_use(pool) -> int:
+    """Bytes of host blocks handed out and not given back (src/plan.jl:322-334);
+    takes the pool or its plan."""
     return sum(_hostpool(pool).cursors) - host_bytes_free(pool)

@@ -131,3 +131,47 @@ def test_tuning_table_is_host_state(fb, tmp_path):
     with pytest.raises(fb.ArgumentError):
         fb.autotune.set_gram_shift(10_000, 16, 9)
     fb.autotune.clear()
+
+
+def test_newer_entry_points_check_arguments_without_a_gpu(fb):
+    # Every check below fires before anything reaches a device: the pointers
+    # are fake (aligned, distinct), never dereferenced.
+    lib = fb._lib.load()
+    E = fb._lib
+    a, b, c, d = 0x10000000, 0x20000000, 0x30000000, 0x40000000
+    n = ctypes.c_size_t(0)
+    # The cholqr2! pullback.
+    assert lib.fb_zcholqr2_adjoint_workspace_size(-1, 4, ctypes.byref(n)) == E.FB_EINVAL
+    assert lib.fb_zcholqr2_adjoint(None, 8, b, 8, c, 4, None, 0, None, 0, 8, 4, None, 0, None) == E.FB_EINVAL
+    assert lib.fb_zcholqr2_adjoint(a, 8, b, 8, c, 4, None, 0, None, 0, -1, 4, None, 0, None) == E.FB_EDIM
+    assert lib.fb_zcholqr2_adjoint(a, 7, b, 8, c, 4, None, 0, None, 0, 8, 4, None, 0, None) == E.FB_EDIM
+    assert lib.fb_zcholqr2_adjoint(a + 8, 8, b, 8, c, 4, None, 0, None, 0, 8, 4, None, 0, None) == E.FB_EINVAL
+    assert lib.fb_zcholqr2_adjoint(a, 8, a + 16 * 8, 8, c, 4, None, 0, None, 0, 8, 4, None, 0, None) == E.FB_EINVAL
+    assert "overlaps" in E.last_error()
+    assert lib.fb_zcholqr2_adjoint(a, 8, b, 8, c, 4, d, 8, None, 0, 8, 4, None, 0, None) == E.FB_ENOMEM
+    # The project pullback.
+    assert lib.fb_zproject_adjoint(None, 8, b, 8, None, 0, c, 4, 8, 4, 0, None, 0, None) == E.FB_EINVAL
+    assert lib.fb_zproject_adjoint(a, 8, b, 8, None, 0, c, 4, -8, 4, 0, None, 0, None) == E.FB_EDIM
+    assert lib.fb_zproject_adjoint(a, 8, a, 8, None, 0, c, 4, 8, 4, 0, None, 0, None) == E.FB_EINVAL
+    # The band operator.
+    assert lib.fb_zhband_apply(a, 8, b, 8, c, 8, -1, 2, 4, None) == E.FB_EINVAL
+    assert lib.fb_zhband_apply(a, 7, b, 8, c, 8, 8, 2, 4, None) == E.FB_EDIM
+    assert lib.fb_zhband_apply(a + 8, 8, b, 8, c, 8, 8, 2, 4, None) == E.FB_EINVAL
+    assert lib.fb_zhband_apply(a, 8, a + 16, 8, c, 8, 8, 2, 4, None) == E.FB_EINVAL
+    # The shifted CholeskyQR3 and its forced-shift factorization.
+    for u in (0.0, 1.5, float("nan")):
+        assert lib.fb_zcholqr3_shifted(a, 8, 8, 4, c, 4, u, None, None, None, 0, None) == E.FB_EINVAL
+        assert lib.fb_zpotrf_forced_shift(a, 4, b, 4, 4, 8, None, 4, None, 4, u, None, None, 0, None) == E.FB_EINVAL
+    # The batch.
+    assert lib.fb_zcholqr2_batched(None, None, None, None, None, None, 0, 0, None, 0, None) == E.FB_OK
+    assert lib.fb_zcholqr2_batched(None, None, None, None, None, None, 2, 0, None, 0, None) == E.FB_EINVAL
+    Ns = (ctypes.c_int64 * 2)(100, 0)
+    ks = (ctypes.c_int * 2)(4, 4)
+    assert lib.fb_zcholqr2_batched_workspace_size(ctypes.cast(Ns, ctypes.c_void_p), ctypes.cast(ks, ctypes.c_void_p),
+                                                   2, ctypes.byref(n)) == E.FB_EINVAL
+    assert "instance 1" in E.last_error()
+    # The tuning table.
+    assert lib.fb_tune_set_batch_lanes(0) == E.FB_EINVAL
+    assert lib.fb_tune_set_batch_lanes(17) == E.FB_EINVAL
+    assert lib.fb_tune_set_gram_chunks(100, 4, 9) == E.FB_EINVAL
+    assert lib.fb_tune_set_gram_chunks(0, 4, 1) == E.FB_EINVAL

@@ -11,11 +11,12 @@
 // storage, which keeps a column of G contiguous.
 //
 // For kd <= 64 the product runs on the FP64 tensor cores (DMMA m8n8k4 on
-// the real form of the complex product): a CTA owns 128 rows, a warp 8 of
-// them, and the band of those 8 rows, columns i - kd .. i + 7 + kd, is the
-// MMA A operand (entries of G, loaded once per k-step and reused for every
-// n-tile) against the real form of X as the B operand. The X rows the CTA's
-// band reaches (128 + 2 kd of them) are staged in shared memory 32 columns at
+// the real form of the complex product): a CTA owns 256 rows, a warp 16 of
+// them (two 8-row m-tiles), and the band of those rows, columns
+// i - kd .. i + 15 + kd, is the MMA A operand (entries of G, loaded once per
+// k-step and reused for every n-tile) against the real form of X as the B
+// operand, each B entry serving both m-tiles. The X rows the CTA's band
+// reaches (256 + 2 kd of them) are staged in shared memory 32 columns at
 // a time, column-major with a padded column length so that one fragment load
 // (two rows by four columns) touches 32 distinct banks. A wider band falls
 // back to the FP64-pipe kernel below: a thread owns one row and CB columns of
@@ -68,13 +69,15 @@ hband_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, int64_
     }
 }
 
-constexpr int HBT_ROWS = 128;             // rows a CTA owns
-constexpr int HBT_WARPS = HBT_ROWS / 8;    // warps, 8 rows each
+constexpr int HBT_MT = 2;                  // 8-row m-tiles a warp owns
+constexpr int HBT_WROWS = 8 * HBT_MT;      // rows a warp owns
+constexpr int HBT_WARPS = 16;
+constexpr int HBT_ROWS = HBT_WARPS * HBT_WROWS;  // rows a CTA owns
 constexpr int HBT_COLS = 32;               // columns of X staged at a time (8 n-tiles)
 constexpr int HBT_KDMAX = 64;
-constexpr int HBT_AHEAD = 4;               // k-steps of band entries loaded ahead
+constexpr int HBT_AHEAD = 2;               // k-steps of band entries loaded ahead (32 products)
 
-// Column length of the staged X tile: 128 + 2 kd rows, padded to 2 mod 8 so
+// Column length of the staged X tile: HBT_ROWS + 2 kd rows, padded to 2 mod 8 so
 // that the four columns a fragment load reads start 8 banks apart.
 __host__ __device__ inline int hbt_pitch(int kd) {
     int r = HBT_ROWS + 2 * kd;
@@ -110,13 +113,12 @@ hband_dmma_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, i
     // for (p, o) = (1, 0): the real form of the complex product.
     const int bpart = p ^ o;
     const double bsign = (p == 1 && o == 0) ? -1.0 : 1.0;
-    const int nsteps = kd + 4;                     // k-steps of an 8-row band: 2 kd + 8 columns
+    const int nsteps = kd + HBT_WROWS / 2;         // k-steps of a warp's band: 2 kd + 16 columns
     const int64_t tiles = (N + HBT_ROWS - 1) / HBT_ROWS;
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t i0 = tile * HBT_ROWS;
         const int64_t xrow0 = i0 - kd;             // first staged row (may be negative: zeros)
-        const int64_t wi0 = i0 + 8 * warp;         // this warp's first row
-        const int64_t row = wi0 + rr;
+        const int64_t wi0 = i0 + HBT_WROWS * warp; // this warp's first row
         for (int c0 = 0; c0 < cols; c0 += HBT_COLS) {
             __syncthreads();   // the previous chunk's fragments have all been read
             for (int e = threadIdx.x; e < staged * HBT_COLS; e += blockDim.x) {
@@ -127,44 +129,67 @@ hband_dmma_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, i
                 xs[c * pitch + r] = v;
             }
             __syncthreads();
-            double acc[8][2];
+            double acc[HBT_MT][8][2];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = 0.0;
+            for (int m = 0; m < HBT_MT; ++m)
+#pragma unroll
+                for (int t = 0; t < 8; ++t) acc[m][t][0] = acc[m][t][1] = 0.0;
             if (wi0 < N) {
-                // k-step s covers columns jb, jb + 1 with jb = wi0 - kd + 2 s;
-                // this lane's A entry is G[row][jb + (kr >> 1)], part p. The
+                // k-step s covers columns jb, jb + 1 with jb = wi0 - kd + 2 s
+                // (the union of the m-tiles' bands); this lane's A entry of
+                // m-tile m is G[wi0 + 8 m + rr][jb + (kr >> 1)], part p. The
                 // entries of the next HBT_AHEAD steps are in flight.
                 const double* dg = reinterpret_cast<const double*>(Dg);
                 const int64_t j0 = wi0 - kd + (kr >> 1);
-                double ring[HBT_AHEAD];
+                double ring[HBT_MT][HBT_AHEAD];
 #pragma unroll
-                for (int q = 0; q < HBT_AHEAD; ++q) ring[q] = band_part(dg, lddg, N, kd, row, j0 + 2 * q, p);
+                for (int m = 0; m < HBT_MT; ++m)
+#pragma unroll
+                    for (int q = 0; q < HBT_AHEAD; ++q)
+                        ring[m][q] = band_part(dg, lddg, N, kd, wi0 + 8 * m + rr, j0 + 2 * q, p);
                 // One k-step against the eight n-tiles: B is rows jb + (kr >> 1)
-                // of the staged tile, columns 4 t + (nr >> 1).
-                auto step = [&](int st, double a) {
+                // of the staged tile, columns 4 t + (nr >> 1); each B entry
+                // serves every m-tile.
+                auto step = [&](int st, const double (&a)[HBT_MT]) {
                     const int lr = (int)(wi0 - xrow0) - kd + 2 * st + (kr >> 1);
                     const double* xb = reinterpret_cast<const double*>(xs + (nr >> 1) * pitch + lr) + bpart;
 #pragma unroll
-                    for (int t = 0; t < 8; ++t) dmma_884(acc[t][0], acc[t][1], a, bsign * xb[2 * (4 * t) * pitch]);
+                    for (int t = 0; t < 8; ++t) {
+                        const double b = bsign * xb[2 * (4 * t) * pitch];
+#pragma unroll
+                        for (int m = 0; m < HBT_MT; ++m) dmma_884(acc[m][t][0], acc[m][t][1], a[m], b);
+                    }
                 };
                 int s = 0;
                 for (; s + HBT_AHEAD <= nsteps; s += HBT_AHEAD) {
 #pragma unroll
                     for (int q = 0; q < HBT_AHEAD; ++q) {
-                        const double a = ring[q];
-                        ring[q] = band_part(dg, lddg, N, kd, row, j0 + 2 * (s + q + HBT_AHEAD), p);
+                        double a[HBT_MT];
+#pragma unroll
+                        for (int m = 0; m < HBT_MT; ++m) {
+                            a[m] = ring[m][q];
+                            ring[m][q] = band_part(dg, lddg, N, kd, wi0 + 8 * m + rr, j0 + 2 * (s + q + HBT_AHEAD), p);
+                        }
                         step(s + q, a);
                     }
                 }
 #pragma unroll
                 for (int q = 0; q < HBT_AHEAD; ++q)
-                    if (s + q < nsteps) step(s + q, ring[q]);
+                    if (s + q < nsteps) {
+                        double a[HBT_MT];
+#pragma unroll
+                        for (int m = 0; m < HBT_MT; ++m) a[m] = ring[m][q];
+                        step(s + q, a);
+                    }
             }
-            if (row < N) {
+#pragma unroll
+            for (int m = 0; m < HBT_MT; ++m) {
+                const int64_t row = wi0 + 8 * m + rr;
+                if (row >= N) continue;
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
                     const int col = c0 + 4 * t + cq;
-                    if (col < cols) Y[row + (int64_t)col * ldy] = zmake(acc[t][0], acc[t][1]);
+                    if (col < cols) Y[row + (int64_t)col * ldy] = zmake(acc[m][t][0], acc[m][t][1]);
                 }
             }
         }

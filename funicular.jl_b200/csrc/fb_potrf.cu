@@ -102,11 +102,14 @@ potrf_kernel(const z64* __restrict__ G, int64_t ldg, int k, int64_t N,
             }
             __syncthreads();
             if (tid == 0) W[j * k + j] = zmake(rj, 0.0);
-            const int n = k - j - 1;
-            for (int t = tid; t < n * n; t += nt) {
-                int m = j + 1 + t / n, l = j + 1 + t % n;
-                if (m <= l) {
-                    z64 a = W[j * k + m], b = W[j * k + l];
+            // The trailing upper triangle: a warp per row m, its lanes along
+            // the row's columns l >= m (each entry updated once per step, so
+            // the order across entries does not reach the bits).
+            const int warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
+            for (int m = j + 1 + warp; m < k; m += nwarps) {
+                const z64 a = W[j * k + m];
+                for (int l = m + lane; l < k; l += 32) {
+                    const z64 b = W[j * k + l];
                     z64 w = W[m * k + l];
                     // w -= conj(a) * b
                     w.x = fma(-a.x, b.x, w.x);

@@ -126,7 +126,9 @@ trsm_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, TrsmPlan* plan, 
         }
         __syncthreads();
     }
-    // 1-norms of R's own columns and of inv(R)'s.
+    // 1-norms of R's own columns and of inv(R)'s, and of the columns of
+    // their 8 x 8 diagonal blocks: a thread per column, each sum in row order.
+    __shared__ double bcolr[TR_KMAX], bcoli[TR_KMAX];
     if (tid < KP) {
         double a = 0.0, b = 0.0;
         for (int i = 0; i <= tid; ++i) {
@@ -135,6 +137,13 @@ trsm_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, TrsmPlan* plan, 
         }
         colr[tid] = tid < k ? a : 0.0;
         coli[tid] = tid < k ? b : 0.0;
+        double cr = 0.0, ci = 0.0;
+        for (int i = TR_NB * (tid / TR_NB); i <= tid; ++i) {
+            cr += hypot(Rs[i * LD + tid].x, Rs[i * LD + tid].y);
+            ci += hypot(Xs[i * LD + tid].x, Xs[i * LD + tid].y);
+        }
+        bcolr[tid] = cr;
+        bcoli[tid] = ci;
     }
     __syncthreads();
     if (tid == 0) {
@@ -148,13 +157,8 @@ trsm_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, TrsmPlan* plan, 
         for (int b = 0; b < KP / TR_NB; ++b) {
             double br = 0.0, bi = 0.0;
             for (int j = TR_NB * b; j < TR_NB * b + TR_NB; ++j) {
-                double cr = 0.0, ci = 0.0;
-                for (int i = TR_NB * b; i <= j; ++i) {
-                    cr += hypot(Rs[i * LD + j].x, Rs[i * LD + j].y);
-                    ci += hypot(Xs[i * LD + j].x, Xs[i * LD + j].y);
-                }
-                br = fmax(br, cr);
-                bi = fmax(bi, ci);
+                br = fmax(br, bcolr[j]);
+                bi = fmax(bi, bcoli[j]);
             }
             worst = fmax(worst, br * bi);
         }

@@ -59,8 +59,14 @@ def parse_args():
                    help="instances of the batched cholqr2! measurement (0 skips it)")
     p.add_argument("--wide-N", type=int, default=10_000_000,
                    help="rows of the k = 128 configuration (0 skips it)")
-    p.add_argument("--rf-k", type=int, default=24, help="columns of the streamed range finder (0 skips it)")
-    p.add_argument("--rf-budget-gib", type=int, default=12, help="device budget of the streamed range finder")
+    p.add_argument("--rf-k", type=int, default=64, help="columns of the streamed range finder (0 skips it)")
+    p.add_argument("--rf-budget-gb", type=float, default=40.0, help="device budget of the streamed range finder, GB")
+    p.add_argument("--project-k", type=int, default=64,
+                   help="columns of the device-resident project on the 215^3 Laplacian (0 skips it)")
+    p.add_argument("--c1-N", type=int, default=1 << 20,
+                   help="rows of the GhostPanels configuration (k = 32, panel width 8; 0 skips it)")
+    p.add_argument("--skip-full-compare", action="store_true",
+                   help="skip the full-size comparison of R and Q with the oracle's in the CPU leg")
     p.add_argument("--adjoint-N", type=int, default=1 << 22,
                    help="rows of the differentiation workload (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace",
@@ -122,6 +128,54 @@ def cpu_cholqr2_rate(Y0: np.ndarray, steps: int, warmup: int):
         times.append(time.perf_counter() - t0)
     sec = statistics.mean(times)
     return alg_bytes(N, k) / sec / 1e9, sec
+
+
+def compare_c1_with_oracle(A, Q, R):
+    """The oracle's cholqr2! (the reference's CPU backend path) on the ghost
+    matrix's entries from the C restatement of the fill, against the device
+    path's Q and R: the entries bit for bit, Q and R to 1e-12 relative."""
+    from oracle import ghost as ghost_oracle
+    from oracle import panel_oracle as oracle
+    N, k = A.shape
+    entries = ghost_oracle.ghost_block(np.complex128, N, k, 0, 0, C1_SEED)
+    same_entries = bool(np.array_equal(entries, A))
+    Qo = entries.copy(order="F")
+    t0 = time.perf_counter()
+    Ro, passes = oracle.cholqr2(Qo, C1_W)
+    sec = time.perf_counter() - t0
+    return {"entries_bitwise_equal": same_entries, "oracle_passes": passes, "oracle_s": sec,
+            "q_rel": float(np.linalg.norm(Q - Qo) / np.linalg.norm(Qo)),
+            "r_rel": float(np.linalg.norm(R - Ro) / np.linalg.norm(Ro)),
+            "orthogonality_fro": oracle.orthogonality_error(Q),
+            "reconstruction_rel": oracle.reconstruction_error(entries, Q, R),
+            "oracle_orthogonality_fro": oracle.orthogonality_error(Qo), "bound_rel": 1e-12,
+            "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13}
+
+
+def compare_full_size_with_oracle(fb, backend, torch, Yt0, Yt, Y, R, queue, stream, N, k):
+    """One cholqr2! of the full-size workload on the device and the oracle's
+    on the same host copy of Y (all host cores): R and Q relative
+    differences. Y's condition number is 1e6, so both factors are determined
+    by Y only to about kappa * eps: the differences are reported against that
+    scale, not against 1e-12."""
+    from oracle import panel_oracle as oracle
+    with torch.cuda.stream(stream):
+        Yt.copy_(Yt0)
+    stream.synchronize()
+    backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, R))
+    Q = Y.to_host()
+    Rh = R.to_host()
+    Yh = np.asfortranarray(wrap(fb, Yt0, N, k).to_host())
+    t0 = time.perf_counter()
+    Ro, passes = oracle.cholqr2(Yh, W_PANEL)
+    sec = time.perf_counter() - t0
+    out = {"N": N, "k": k, "oracle_s": sec, "oracle_passes": passes, "kappa": 1e6,
+           "r_rel": float(np.linalg.norm(Rh - Ro) / np.linalg.norm(Ro)),
+           "q_rel": float(np.linalg.norm(Q - Yh) / np.linalg.norm(Yh)),
+           "oracle_orthogonality_fro": oracle.orthogonality_error(Yh),
+           "scale_kappa_eps": 1e6 * 2.0 ** -52}
+    del Q, Yh
+    return out
 
 
 def synthetic_host_sample(rows, k, seed=0xDEADBEEF):
@@ -225,7 +279,7 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier):
+def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak):
     """The batched range finder's orthonormalization: args.batch independent
     cholqr2! instances, N log-uniform on [1e4, 2e6], k drawn from {16, 32, 64}
     (seeded), all enqueued by one fb_zcholqr2_batched call, timed eagerly and
@@ -277,6 +331,10 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
     ms_eager = timed(eager)
     ms_graph = timed(lambda: graph.launch(queue))
     alg = float(sum(96.0 * N * k for N, k in zip(Ns, ks)))
+    # The batch's roofline: each instance at the slower of its HBM time
+    # (96 N k bytes) and its FP64 time (16 N k^2 flops), summed.
+    roof_ms = float(sum(max(96.0 * N * k / (hbm_peak * 1e9), 16.0 * N * k * k / (fp64_peak * 1e12))
+                        for N, k in zip(Ns, ks))) * 1e3
     del graph
     # The same batch after the autotuner has chosen the Gram's row chunks for
     # each shape class of the batch (each class tuned at its largest N).
@@ -301,9 +359,87 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
                       "ms_by_lanes_eager": lanes["ms"], "tuning_s": tune_s,
                       "passes_max": max(passes_t)},
             "alg_bytes_per_step": alg, "ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
+            "roofline": {"ms": roof_ms, "frac_graph": roof_ms / ms_graph, "frac_eager": roof_ms / ms_eager,
+                         "rule": "sum over instances of max(96 N k / HBM peak, 16 N k^2 / FP64 peak)"},
             "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
             "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,
             "launch": "one fb_zcholqr2_batched call (eight stream lanes), replayed as one captured CUDA graph"}
+
+
+C1_K, C1_W, C1_SEED = 32, 8, 0xDEADBEEF
+
+
+def run_c1(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak):
+    """The GhostPanels configuration: cholqr2! of a PanelMatrix{ComplexF64}
+    with N = 2^20 rows, k = 32 columns and panel width 8, copied from
+    GhostPanels(ComplexF64, N, k; seed = 0xdeadbeef) (filled on the device).
+    End to end through the public API (copyto!(Y, Omega), then cholqr2(Y) on
+    the page-locked host panels, resident since Y fits), and the device chain
+    alone with the ghost fill restoring Y before each step, outside the step's
+    event pair. Returns the record and the host input, Q and R for the
+    oracle comparison of the CPU leg."""
+    N, k, w = args.c1_N, C1_K, C1_W
+    nbytes = N * k * 16
+    plan = fb.ResidencyPlan(device_budget=4 * nbytes + fb.GiB, host_budget=2 * nbytes + 64 * 2 ** 20,
+                            backend=backend)
+    Omega = fb.GhostPanels(np.complex128, N, k, plan=plan, seed=C1_SEED, w=w)
+    Y = fb.PanelMatrix.undef(np.complex128, N, k, plan=plan, w=w)
+    Y.copy_from(Omega)
+    A = Y.to_array()
+    times = []
+    for i in range(args.e2e_steps + 1):
+        Y.copy_from(A)
+        barrier()
+        t0 = time.perf_counter()
+        R = fb.cholqr2(Y)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            times.append(dt)
+    Q = Y.to_array()
+    ms_e2e = max_over_ranks(1e3 * sum(times) / max(1, len(times)))
+    fb.free(Y)
+
+    # The device chain alone: the ghost fill regenerates Y, then one event
+    # pair around cholqr2!.
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    D = backend.alloc_device(np.complex128, (N, k))
+    Rd = backend.alloc_device(np.complex128, (k, k))
+
+    def fill():
+        backend.submit(queue, lambda: fb.kernels.ghost_fill(backend, D, 0, 0, C1_SEED, np.complex128))
+
+    def step():
+        backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, D, Rd, wait=False))
+
+    for _ in range(max(3, args.warmup)):
+        fill()
+        step()
+    backend.sync_queue(queue)
+    barrier()
+    pairs = []
+    for _ in range(args.steps):
+        fill()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        pairs.append((a, b))
+    pairs[-1][1].synchronize()
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in pairs)) / args.steps
+    roof_ms = max(alg_bytes(N, k) / (hbm_peak * 1e9), alg_flops(N, k) / (fp64_peak * 1e12)) * 1e3
+    record = {
+        "workload": f"cholqr2! of PanelMatrix{{ComplexF64}} N={N}, k={k}, panel width {w}, copied from "
+                    f"GhostPanels seed {C1_SEED:#x} (device fill)",
+        "ms_per_step": ms, "value": whole_job_gbs(alg_bytes(N, k), world, ms), "unit": UNIT,
+        "step_roofline": {"ms_roofline": roof_ms, "frac": roof_ms / ms},
+        "e2e": {"ms_per_step": ms_e2e, "value": whole_job_gbs(alg_bytes(N, k), world, ms_e2e), "unit": UNIT,
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + k * k * 16,
+                "path": "Y.copy_from(A); funicular_b200.cholqr2(Y) on page-locked host panels"},
+    }
+    del D, Rd
+    return record, (A, Q, R)
 
 
 def run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak):
@@ -447,13 +583,16 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
     grid = (342, 342, 342)
     N = grid[0] * grid[1] * grid[2]
     k = args.rf_k
-    # Host blocks are whole panels of the plan's width (the last one too).
-    plan = fb.ResidencyPlan(device_budget=args.rf_budget_gib * fb.GiB, host_budget=int(1.5 * N * k * 16) + 4 * fb.GiB,
-                            backend=backend)
+    # Host blocks are whole panels of the plan's width (the last one too);
+    # room for Y and for project's second matrix Z (the two-sweep schedule).
+    budget = int(args.rf_budget_gb * 1e9)
+    plan = fb.ResidencyPlan(device_budget=budget, host_budget=int(2.1 * N * k * 16) + 4 * fb.GiB, backend=backend)
     X = fb.GhostPanels(np.complex128, N, k, plan=plan, seed=0xC4)
     Y = fb.PanelMatrix.undef(np.complex128, N, k, plan=plan, w=X.w)
     G = fb.Laplacian7(grid, 0.5 + 0.1j)
     pcie = measure_pcie(torch, device)
+
+    schedule = fb.panelblas.project_schedule(Y)
 
     def step():
         t = [time.perf_counter()]
@@ -461,7 +600,7 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
         t.append(time.perf_counter())
         R = fb.cholqr2(Y, resident=False)
         t.append(time.perf_counter())
-        S = fb.project(Y, G)
+        S = fb.project(Y, G, schedule=schedule)
         t.append(time.perf_counter())
         return [1e3 * (t[i + 1] - t[i]) for i in range(3)], R, S
 
@@ -476,9 +615,16 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
     passes = 2  # the third pass runs only after a shift, and the Gram of G X is well conditioned here
     # Host to device and back, per phase: panelmul writes Y (X is generated on
     # the device); a cholqr2 pass reads Y twice (Gram, solve) and writes it
-    # once; project uploads p (p + 1) panels.
-    up = {"panelmul": 0, "cholqr2": passes * 2 * col * k, "project": col * sum(widths) + col * p * sum(widths)}
-    down = {"panelmul": col * k, "cholqr2": passes * col * k, "project": 0}
+    # once; project in two sweeps reads Y, writes Z = G Y, then reads both
+    # (the nested schedule uploads p (p + 1) panels).
+    if schedule == "two-sweep":
+        up_project, down_project = 3 * col * k, col * k
+    elif schedule == "resident":
+        up_project, down_project = col * k, 0
+    else:
+        up_project, down_project = col * sum(widths) + col * p * sum(widths), 0
+    up = {"panelmul": 0, "cholqr2": passes * 2 * col * k, "project": up_project}
+    down = {"panelmul": col * k, "cholqr2": passes * col * k, "project": down_project}
     Gq = fb.gram(Y)
     orth = float(np.linalg.norm(Gq - np.eye(k)))
     total_ms = sum(ms)
@@ -487,7 +633,9 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
     # direction's bytes over its measured bandwidth.
     bound_ms = 1e3 * max(sum(up.values()) / (pcie["h2d"] * 1e9), sum(down.values()) / (pcie["d2h"] * 1e9))
     out = {"workload": f"streamed range finder, 342^3 Laplacian (N={N}), k={k}, {p} panels of width {max(widths)}, "
-                       f"device budget {args.rf_budget_gib} GiB for a {col * k / 1e9:.1f} GB matrix",
+                       f"device budget {budget / 1e9:.1f} GB for a {col * k / 1e9:.1f} GB matrix, "
+                       f"project schedule {schedule}",
+           "project_schedule": schedule,
            "ms": {"panelmul": ms[0], "cholqr2_streamed": ms[1], "project": ms[2], "step": total_ms},
            "bus_bytes_up": up, "bus_bytes_down": down, "bus_gbs": total_bus / (total_ms * 1e-3) / 1e9,
            "pcie_measured_gbs": pcie, "ms_pcie_bound": bound_ms, "pcie_roofline_frac": bound_ms / total_ms,
@@ -496,6 +644,73 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
     fb.free(Y)
     del X, Y, plan
     return out
+
+
+def run_project(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak):
+    """project(Q, G) = Q^H (G Q) device-resident (src/panelblas.jl:268-301 in
+    its two-sweep form): Q is N x k with N = 215^3 = 9 938 375 (the C2 size on
+    a cube), k = args.project_k, G = -Lap_7 + (0.5+0.1i) I. Timed on the
+    device: the operator applied to all of Q, the cross Gram Q^H (G Q) (the
+    projection proper: 32 N k bytes, 8 N k^2 flops), and both; end to end:
+    project() on a PanelMatrix in page-locked host panels (Q up once, G
+    applied, one cross Gram, S to the host)."""
+    grid = (215, 215, 215)
+    N = grid[0] * grid[1] * grid[2]
+    k = args.project_k
+    G = fb.Laplacian7(grid, 0.5 + 0.1j)
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    Q = backend.alloc_device(np.complex128, (N, k))
+    Z = backend.alloc_device(np.complex128, (N, k))
+    S = backend.alloc_device(np.complex128, (k, k))
+    backend.submit(queue, lambda: fb.kernels.ghost_fill(backend, Q, 0, 0, 0x9A0, np.complex128))
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            backend.submit(queue, fn)
+        backend.sync_queue(queue)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            backend.submit(queue, fn)
+        b.record(stream)
+        b.synchronize()
+        return max_over_ranks(a.elapsed_time(b) / args.steps)
+
+    ms_apply = timed(lambda: G.apply(backend, Z, Q))
+    ms_gram = timed(lambda: fb.kernels.gram_accumulate(backend, S, Q, Z, 1.0, 0.0))
+    ms_both = timed(lambda: (G.apply(backend, Z, Q), fb.kernels.gram_accumulate(backend, S, Q, Z, 1.0, 0.0)))
+    flops, nbytes = 8 * N * k * k, 32 * N * k
+    roof_ms = max(nbytes / (hbm_peak * 1e9), flops / (fp64_peak * 1e12)) * 1e3
+    # End to end through the public API.
+    Qh = np.asfortranarray(Q.to_host())
+    plan = fb.ResidencyPlan(device_budget=3 * N * k * 16 + fb.GiB, host_budget=N * k * 16 + 64 * 2 ** 20,
+                            backend=backend, panel_width=16)
+    Qpm = fb.PanelMatrix.from_array(Qh, plan=plan)
+    schedule = fb.panelblas.project_schedule(Qpm)
+    times = []
+    for i in range(4):
+        barrier()
+        t0 = time.perf_counter()
+        Sh = fb.project(Qpm, G)
+        if i:
+            times.append(time.perf_counter() - t0)
+    ms_e2e = max_over_ranks(1e3 * sum(times) / len(times))
+    fb.free(Qpm)
+    del Qh, Qpm, plan, Q, Z
+    return {"workload": f"project(Q, G), N={N} (215^3 Laplacian, shift 0.5+0.1i), k={k}, device-resident",
+            "cross_gram": {"ms": ms_gram, "tflops": flops / (ms_gram * 1e-3) / 1e12,
+                           "gbs": nbytes / (ms_gram * 1e-3) / 1e9, "ms_roofline": roof_ms, "frac": roof_ms / ms_gram,
+                           "per_launch": "8 N k^2 flops, 32 N k bytes (Q and G Q read)"},
+            "apply": {"ms": ms_apply, "gbs": 32 * N * k / (ms_apply * 1e-3) / 1e9,
+                      "hbm_frac": 32 * N * k / (ms_apply * 1e-3) / 1e9 / hbm_peak,
+                      "per_launch": "32 N k bytes (Q read, G Q written)"},
+            "ms_apply_plus_gram": ms_both,
+            "e2e": {"ms_per_call": ms_e2e, "schedule": schedule, "h2d_bytes": N * k * 16,
+                    "path": "funicular_b200.project(PanelMatrix, Laplacian7) on page-locked host panels",
+                    "s_finite": bool(np.isfinite(Sh).all())}}
 
 
 def run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier):
@@ -735,27 +950,43 @@ def run_ours(args):
     def step():
         backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, R, wait=False))
 
+    def restore():
+        # Every step orthonormalizes the configured input, not the Q the
+        # previous step left: a device-to-device copy of the pristine Y on the
+        # queue, outside the step's event pair.
+        with torch.cuda.stream(stream):
+            Yt.copy_(Yt0)
+
+    def timed_steps(fn, count, with_launches=False):
+        """count steps, each on a freshly restored Y, every step bracketed by
+        its own CUDA-event pair on the queue; returns (summed ms, launches)."""
+        pairs = []
+        launches_before = fb._lib.kernel_launches()
+        for _ in range(count):
+            restore()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            pairs.append((a, b))
+        pairs[-1][1].synchronize()
+        return sum(a.elapsed_time(b) for a, b in pairs), fb._lib.kernel_launches() - launches_before
+
     for _ in range(args.warmup):
+        restore()
         step()
     backend.sync_queue(queue)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
 
-    launches0 = fb._lib.kernel_launches()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
-        e1.synchronize()
-    launches = fb._lib.kernel_launches() - launches0
+        ms_total, launches = timed_steps(step, args.steps)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_total = max_over_ranks(ms_total)
     ms_step = ms_total / args.steps
     value = whole_job_gbs(alg_bytes(N, k) * args.steps, world, ms_total)
 
@@ -777,18 +1008,13 @@ def run_ours(args):
             backend.submit(queue, lambda: fb.kernels.cholqr2_resident(backend, Y, Rtc, wait=False, form="tc"))
 
         for _ in range(args.warmup):
+            restore()
             step_tc()
         backend.sync_queue(queue)
         barrier()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        for _ in range(args.steps):
-            step_tc()
-        t1.record(stream)
-        t1.synchronize()
+        ms_tc_total, _ = timed_steps(step_tc, args.steps)
         barrier()
-        ms_tc = max_over_ranks(t0.elapsed_time(t1)) / args.steps
+        ms_tc = max_over_ranks(ms_tc_total) / args.steps
         tensor_form = {
             "ms_per_step": ms_tc, "value": world * alg_bytes(N, k) / (ms_tc * 1e-3) / 1e9, "unit": UNIT,
             "speedup_vs_fp64_form": ms_step / ms_tc, "passes": passes_tc,
@@ -824,6 +1050,15 @@ def run_ours(args):
     R1 = backend.todevice(np.asfortranarray(R.to_host()))
     trsm_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.rdiv_upper(backend, Y, Rid)), reps)
     trsm_blocked_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.rdiv_upper(backend, Y, R1)), reps)
+    # rightmul_gemm! (src/kernels.jl:73, the product behind rightmul! and the
+    # dense operator): Z <- Y C with a dense k x k C, into a second N x k
+    # buffer. 8 N k^2 flops (a full complex product), 32 N k bytes.
+    Zt = torch.empty_like(Yt)
+    torch.cuda.synchronize()
+    Zm = wrap(fb, Zt, N, k)
+    rightmul_ms = time_kernel(lambda: backend.submit(queue, lambda: fb.kernels.rightmul_gemm(backend, Zm, Y, R1)),
+                              reps)
+    del Zm, Zt
     # The GhostPanels device fill (the C1 input generator), over the same
     # N x k block: 16 N k bytes written per launch, nothing read. It runs last
     # because it overwrites Y.
@@ -839,6 +1074,10 @@ def run_ours(args):
                          "gbs": 32 * N * k / (trsm_blocked_ms * 1e-3) / 1e9},
     }
     dominant = max(kernels, key=lambda name: kernels[name]["ms"])
+    kernels["rightmul_gemm"] = {"ms": rightmul_ms, "tflops": 8 * N * k * k / (rightmul_ms * 1e-3) / 1e12,
+                                "gbs": 32 * N * k / (rightmul_ms * 1e-3) / 1e9,
+                                "fp64_frac": 8 * N * k * k / (rightmul_ms * 1e-3) / 1e12 / fp64_peak,
+                                "per_launch": f"8 N k^2 = {8 * N * k * k:.3e} flops, 32 N k bytes"}
     if gram_tc_ms is not None:
         kernels["gram_tensor_cores"] = {"ms": gram_tc_ms, "tflops": kernel_flops / (gram_tc_ms * 1e-3) / 1e12,
                                         "gbs": 16 * N * k / (gram_tc_ms * 1e-3) / 1e9,
@@ -865,7 +1104,10 @@ def run_ours(args):
         "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_source, "fp64_peak_tflops": fp64_peak,
     }
 
-    batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier)
+    c1, c1_outputs = (run_c1(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
+                      if args.c1_N > 0 else (None, None))
+
+    batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
                if args.batch > 0 else None)
 
     wide = (run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak)
@@ -874,6 +1116,8 @@ def run_ours(args):
         wide["storage"] = run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, barrier)
     range_finder = (run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                     if args.rf_k > 0 else None)
+    project = (run_project(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
+               if args.project_k > 0 else None)
     adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
                if args.adjoint_N > 0 else None)
     if adjoint is not None:
@@ -917,12 +1161,22 @@ def run_ours(args):
         del Yhost, Ypm, plan
 
     cpu = None
+    full_compare = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         rows = min(N, CPU_SAMPLE_ROWS)
         sample = np.asfortranarray(wrap(fb, Yt0, N, k).view(slice(0, rows)).to_host())
         gbs, sec = cpu_cholqr2_rate(sample, steps=2, warmup=0)
         cpu = {"value": gbs, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
                "sample": f"first {rows} rows of the workload (k={k}), 2 timed steps of {sec:.3f} s each"}
+        del sample
+        # The oracle as the checker: the GhostPanels configuration's Q and R
+        # against the oracle's on the same entries (its C restatement of the
+        # ghost fill), and the full-size workload's R and Q against the
+        # oracle's full-size run.
+        if c1_outputs is not None:
+            c1["oracle"] = compare_c1_with_oracle(*c1_outputs)
+        if not args.skip_full_compare:
+            full_compare = compare_full_size_with_oracle(fb, backend, torch, Yt0, Yt, Y, R, queue, stream, N, k)
 
     if world > 1:
         dist.barrier()
@@ -937,8 +1191,11 @@ def run_ours(args):
         "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
         "accuracy": {"orthogonality_fro": orth, "orthogonality_fro_cublas": orth_cublas,
                      "reconstruction_rel": recon, "passes": passes,
-                     "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13},
+                     "bound_orthogonality": 1e-12, "bound_reconstruction": 1e-13,
+                     "vs_oracle_full_size": full_compare},
+        "c1": c1,
         "tensor_form": tensor_form, "batched": batched, "wide": wide, "range_finder": range_finder, "adjoint": adjoint,
+        "project": project,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)

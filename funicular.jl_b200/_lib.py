@@ -104,6 +104,10 @@ SIGNATURES = {
     "fb_zcholqr2_workspace_size": [_i64, _int, _psz],
     "fb_zcholqr2": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zcholqr2_query": [_vp, _pint, _pint, _pdbl],
+    "fb_zcholqr2_staged_blocks": [_i64, _int, _pint],
+    "fb_zcholqr2_staged_workspace_size": [_i64, _int, _int, _psz],
+    "fb_zcholqr2_staged": [_vp, _int, _vp, _vp, _int, _vp, _i64, _i64, _int, _vp, _i64, ctypes.c_double, _pint,
+                           _pint, _vp, _sz, _vp],
     "fb_zcholqr2_tc": [_vp, _i64, _i64, _int, _vp, _i64, _pint, _pint, _vp, _sz, _vp],
     "fb_zgram_tc_workspace_size": [_i64, _int, _psz],
     "fb_zgram_tc": [_vp, _i64, _vp, _i64, _i64, _int, Z128, Z128, _vp, _sz, _vp],
@@ -177,6 +181,13 @@ def call(name: str, *args) -> None:
 def kernel_launches() -> int:
     """Kernels the library has launched in this process."""
     return int(load().fb_kernel_launches())
+
+
+def staged_blocks(N: int, k: int) -> int:
+    """Row blocks fb_zcholqr2_staged moves an N x k matrix in."""
+    n = ctypes.c_int(0)
+    call("fb_zcholqr2_staged_blocks", ctypes.c_int64(N), k, ctypes.byref(n))
+    return n.value
 
 
 def device_count() -> int:

@@ -24,6 +24,12 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
                  void* workspace, size_t workspace_bytes, cudaStream_t stream,
                  const ChainStatus* st, int gate);
 size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian);
+void gram_chunks(int64_t rows, int kA, int kB, bool hermitian, int64_t* chunk_rows, int* nchunks);
+int gram_partials_enqueue(const z64* A, int64_t lda, const z64* B, int64_t ldb, int64_t rows, int kA, int kB,
+                          bool hermitian, void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                          const ChainStatus* st, int gate, int chunk0, int chunk1);
+int gram_reduce_enqueue(z64* C, int64_t ldc, int64_t rows, int kA, int kB, bool hermitian, z64 alpha, z64 beta,
+                        void* workspace, cudaStream_t stream, const ChainStatus* st, int gate);
 int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t ldr, void* workspace,
                  size_t workspace_bytes, cudaStream_t stream, const ChainStatus* st, int gate);
 size_t trsm_workspace_bytes(int k);
@@ -160,6 +166,7 @@ static int cholqr2_chain(fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, 
 // instance. Fork and join are plain event records and waits, so a captured
 // batch is one graph with the lanes as parallel branches.
 constexpr int BATCH_LANES = 16;        // most lanes a batch can use
+constexpr int STAGED_BLOCKS = 8;       // row blocks of the host-staged cholqr2!
 static std::atomic<int> g_batch_lanes{8};  // lanes a batch uses: the autotuner's entry, 8 untuned
 static size_t batch_status_bytes(int count) { return align_up((size_t)count * sizeof(ChainStatus), 256); }
 static int batch_lanes(int count) {
@@ -351,6 +358,273 @@ int fb_tune_get_batch_lanes(int* lanes) {
     if (!lanes) { set_error(FB_EINVAL, "fb_tune_get_batch_lanes: NULL"); return FB_EINVAL; }
     *lanes = g_batch_lanes.load();
     return FB_OK;
+}
+
+// ---- cholqr2! of a matrix held in page-locked host panels -----------------
+//
+// The end-to-end form: the panels go up in row blocks on one stream while the
+// first pass's Gram consumes the blocks that have landed (the Gram's row
+// chunks are grouped into the blocks, so its partial tiles, and with them its
+// bits, are those of one launch over the whole matrix); the chain runs on the
+// device; the last triangular solve runs block by block and each finished
+// block goes down on a second stream while the next is solved. Every result
+// equals fb_zcholqr2's on the same matrix to the bit.
+
+// The up and down streams of the current device, created once.
+static int staging_streams(cudaStream_t* up, cudaStream_t* down) {
+    static std::mutex mu;
+    static cudaStream_t streams[64][2] = {};
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) { set_error(FB_ENOTSUP, "cholqr2! staged: device %d", dev); return FB_ENOTSUP; }
+    std::lock_guard<std::mutex> lock(mu);
+    for (int i = 0; i < 2; ++i)
+        if (!streams[dev][i])
+            FB_CUDA(cudaStreamCreateWithFlags(&streams[dev][i], cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    *up = streams[dev][0];
+    *down = streams[dev][1];
+    return FB_OK;
+}
+
+namespace {
+// Events of one staged call, destroyed when it returns.
+struct EventSet {
+    std::vector<cudaEvent_t> ev;
+    ~EventSet() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    int make(cudaEvent_t* out) {
+        cudaEvent_t e;
+        FB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreateWithFlags");
+        ev.push_back(e);
+        *out = e;
+        return FB_OK;
+    }
+};
+}  // namespace
+
+// Row blocks of a staged call: whole Gram chunks, at most STAGED_BLOCKS.
+struct StagedBlocks {
+    int64_t chunk_rows = 0;
+    int nchunks = 0, nb = 0;
+    std::vector<int> c0;
+    int64_t max_rows = 0;
+    void rows(int b, int64_t N, int64_t* r0, int64_t* r1) const {
+        *r0 = (int64_t)c0[b] * chunk_rows;
+        *r1 = std::min<int64_t>(N, (int64_t)c0[b + 1] * chunk_rows);
+    }
+};
+
+static StagedBlocks staged_blocks(int64_t N, int k) {
+    StagedBlocks B;
+    gram_chunks(N, k, k, true, &B.chunk_rows, &B.nchunks);
+    B.nb = B.nchunks < STAGED_BLOCKS ? B.nchunks : STAGED_BLOCKS;
+    B.c0.resize(B.nb + 1);
+    for (int b = 0; b <= B.nb; ++b) B.c0[b] = (int)((int64_t)B.nchunks * b / B.nb);
+    for (int b = 0; b < B.nb; ++b) {
+        int64_t r0, r1;
+        B.rows(b, N, &r0, &r1);
+        B.max_rows = std::max(B.max_rows, r1 - r0);
+    }
+    return B;
+}
+
+// The chain's workspace, then (for a ComplexF32 host tier) two narrow
+// staging buffers of one row block each.
+static size_t staged_stage_bytes(int64_t N, int k, int host_type) {
+    if (host_type != FB_C64) return 0;
+    return align_up((size_t)staged_blocks(N, k).max_rows * k * 8, 256);
+}
+
+int fb_zcholqr2_staged_blocks(int64_t N, int k, int* blocks) {
+    if (!blocks || N < 1 || k < 1) { set_error(FB_EINVAL, "fb_zcholqr2_staged_blocks: bad argument"); return FB_EINVAL; }
+    *blocks = staged_blocks(N, k).nb;
+    return FB_OK;
+}
+
+int fb_zcholqr2_staged_workspace_size(int64_t N, int k, int host_type, size_t* bytes) {
+    if (!bytes || N < 1 || k < 1 || (host_type != FB_C128 && host_type != FB_C64)) {
+        set_error(FB_EINVAL, "fb_zcholqr2_staged_workspace_size: bad argument");
+        return FB_EINVAL;
+    }
+    *bytes = cholqr_layout(N, k).total + 2 * staged_stage_bytes(N, k, host_type);
+    return FB_OK;
+}
+
+int fb_zcholqr2_staged(void* const* host_panels, int host_type, const int64_t* host_ld, const int* panel_cols,
+                       int npanels, fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr,
+                       double shift_unit_roundoff, int* info, int* passes, void* workspace, size_t workspace_bytes,
+                       fb_queue_t queue) {
+    if (N < 1 || k < 1) {
+        set_error(FB_EINVAL, "cholqr2!: N and k must be positive, got N=%lld, k=%d", (long long)N, k);
+        return FB_EINVAL;
+    }
+    if (!host_panels || !host_ld || !panel_cols || npanels < 1 || !Y || !R) {
+        set_error(FB_EINVAL, "fb_zcholqr2_staged: NULL argument");
+        return FB_EINVAL;
+    }
+    if (host_type != FB_C128 && host_type != FB_C64) {
+        set_error(FB_EINVAL, "fb_zcholqr2_staged: host panels are ComplexF64 (FB_C128) or ComplexF32 (FB_C64), got %d",
+                  host_type);
+        return FB_EINVAL;
+    }
+    if (!(shift_unit_roundoff >= 0.0 && shift_unit_roundoff < 1.0)) {
+        set_error(FB_EINVAL, "fb_zcholqr2_staged: the unit roundoff of the shift must lie in [0, 1), got %g",
+                  shift_unit_roundoff);
+        return FB_EINVAL;
+    }
+    int cols = 0;
+    for (int p = 0; p < npanels; ++p) {
+        if (!host_panels[p] || panel_cols[p] < 1 || host_ld[p] < N) {
+            set_error(FB_EDIM, "fb_zcholqr2_staged: panel %d is NULL, empty or has a leading dimension below N", p);
+            return FB_EDIM;
+        }
+        cols += panel_cols[p];
+    }
+    if (cols != k) {
+        set_error(FB_EDIM, "fb_zcholqr2_staged: the panels hold %d columns, the matrix %d", cols, k);
+        return FB_EDIM;
+    }
+    if (ldy < N || ldr < k) { set_error(FB_EDIM, "fb_zcholqr2_staged: leading dimension too small"); return FB_EDIM; }
+    if (((uintptr_t)Y | (uintptr_t)R) & 15) {
+        set_error(FB_EINVAL, "fb_zcholqr2_staged: device pointers must be 16-byte aligned");
+        return FB_EINVAL;
+    }
+    CholqrLayout L = cholqr_layout(N, k);
+    const size_t stage_bytes = staged_stage_bytes(N, k, host_type);
+    const size_t total = L.total + 2 * stage_bytes;
+    if (!workspace || workspace_bytes < total || ((uintptr_t)workspace & 255)) {
+        set_error(FB_ENOMEM, "fb_zcholqr2_staged: workspace must be 256-byte aligned and hold %zu bytes (got %zu)",
+                  total, workspace_bytes);
+        return FB_ENOMEM;
+    }
+    char* ws = static_cast<char*>(workspace);
+    ChainStatus* st = reinterpret_cast<ChainStatus*>(ws + L.status);
+    z64* G = reinterpret_cast<z64*>(ws + L.G);
+    z64* U = reinterpret_cast<z64*>(ws + L.U);
+    z64* Ra = reinterpret_cast<z64*>(ws + L.Ra);
+    z64* Rb = reinterpret_cast<z64*>(ws + L.Rb);
+    z64* gwork = reinterpret_cast<z64*>(ws + L.gwork);
+    void* gram_ws = ws + L.gram;
+    void* trsm_ws = ws + L.trsm;
+    const size_t trsm_bytes = L.gram - L.trsm;
+    const size_t gram_bytes = L.total - L.gram;
+    char* stage[2] = {ws + L.total, ws + L.total + stage_bytes};
+    cudaStream_t stream = stream_of(queue);
+    z64* Yz = reinterpret_cast<z64*>(Y);
+    const z64 one = zmake(1.0, 0.0), zero = zmake(0.0, 0.0);
+    const bool narrow = host_type == FB_C64;
+    const size_t hsize = narrow ? 8 : 16;
+    cudaStream_t up, down;
+    FB_TRY(staging_streams(&up, &down));
+    const StagedBlocks B = staged_blocks(N, k);
+    const int nb = B.nb;
+    const int64_t sld = B.max_rows;   // leading dimension of a narrow staging block
+
+    // One 2-D copy per panel of row block b, between host panel p (column
+    // major, leading dimension host_ld[p]) and its columns of `dev` (Y
+    // itself, or a narrow staging block whose rows start at r0).
+    auto copy_block = [&](int b, bool to_device, cudaStream_t s) -> int {
+        int64_t r0, r1;
+        B.rows(b, N, &r0, &r1);
+        if (r1 <= r0) return FB_OK;
+        int col = 0;
+        for (int p = 0; p < npanels; ++p) {
+            char* dev = narrow ? stage[b & 1] + (size_t)col * sld * hsize
+                               : reinterpret_cast<char*>(Yz + r0 + (int64_t)col * ldy);
+            const size_t dpitch = narrow ? (size_t)sld * hsize : (size_t)ldy * sizeof(z64);
+            char* host = static_cast<char*>(host_panels[p]) + (size_t)r0 * hsize;
+            const size_t hpitch = (size_t)host_ld[p] * hsize;
+            const size_t width = (size_t)(r1 - r0) * hsize;
+            if (to_device)
+                FB_CUDA(cudaMemcpy2DAsync(dev, dpitch, host, hpitch, width, panel_cols[p], cudaMemcpyHostToDevice, s),
+                        "cudaMemcpy2DAsync");
+            else
+                FB_CUDA(cudaMemcpy2DAsync(host, hpitch, dev, dpitch, width, panel_cols[p], cudaMemcpyDeviceToHost, s),
+                        "cudaMemcpy2DAsync");
+            col += panel_cols[p];
+        }
+        return FB_OK;
+    };
+
+    EventSet events;
+    std::vector<cudaEvent_t> widened(nb), sent(nb);
+    cudaEvent_t start;
+    FB_TRY(events.make(&start));
+    FB_CUDA(cudaMemsetAsync(st, 0, sizeof(ChainStatus), stream), "cudaMemsetAsync");
+    FB_CUDA(cudaEventRecord(start, stream), "cudaEventRecord");
+    FB_CUDA(cudaStreamWaitEvent(up, start, 0), "cudaStreamWaitEvent");
+    // Pass 1's Gram, block by block as the rows land (widened first when the
+    // panels are narrow; a staging block is reused once its widening ran).
+    for (int b = 0; b < nb; ++b) {
+        if (narrow && b >= 2) FB_CUDA(cudaStreamWaitEvent(up, widened[b - 2], 0), "cudaStreamWaitEvent");
+        FB_TRY(copy_block(b, true, up));
+        cudaEvent_t landed;
+        FB_TRY(events.make(&landed));
+        FB_CUDA(cudaEventRecord(landed, up), "cudaEventRecord");
+        FB_CUDA(cudaStreamWaitEvent(stream, landed, 0), "cudaStreamWaitEvent");
+        if (narrow) {
+            int64_t r0, r1;
+            B.rows(b, N, &r0, &r1);
+            FB_TRY(fb_convert_copy(Yz + r0, FB_C128, ldy, stage[b & 1], FB_C64, sld, r1 - r0, k, queue));
+            FB_TRY(events.make(&widened[b]));
+            FB_CUDA(cudaEventRecord(widened[b], stream), "cudaEventRecord");
+        }
+        FB_TRY(gram_partials_enqueue(Yz, ldy, Yz, ldy, N, k, k, true, gram_ws, gram_bytes, stream, st, GATE_HEALTHY,
+                                     B.c0[b], B.c0[b + 1]));
+    }
+    FB_TRY(gram_reduce_enqueue(G, k, N, k, k, true, one, zero, gram_ws, stream, st, GATE_HEALTHY));
+    FB_TRY(potrf_enqueue(G, k, k, N, U, k, nullptr, k, Ra, k, gwork, st, 1, GATE_HEALTHY, stream,
+                         shift_unit_roundoff));
+    FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, trsm_ws, trsm_bytes, stream, st, GATE_HEALTHY));
+    FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st,
+                        GATE_HEALTHY));
+    FB_TRY(potrf_enqueue(G, k, k, N, U, k, Ra, k, Rb, k, gwork, st, 2, GATE_HEALTHY, stream, 0.0));
+    // Whether a third pass runs (or the chain stopped) decides which solve is
+    // the last: read the status once here.
+    ChainStatus hs;
+    FB_CUDA(cudaMemcpyAsync(&hs, st, sizeof(ChainStatus), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync");
+    FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    const bool third = !hs.failed && (hs.shifted[1] | hs.shifted[2]);
+    if (third) {
+        FB_TRY(trsm_enqueue(Yz, ldy, N, k, U, k, trsm_ws, trsm_bytes, stream, st, GATE_HEALTHY));
+        FB_TRY(gram_enqueue(G, k, Yz, ldy, Yz, ldy, N, k, k, one, zero, true, gram_ws, gram_bytes, stream, st,
+                            GATE_HEALTHY));
+        FB_TRY(potrf_enqueue(G, k, k, N, U, k, Rb, k, Ra, k, gwork, st, 3, GATE_HEALTHY, stream, 0.0));
+        FB_CUDA(cudaMemcpyAsync(&hs, st, sizeof(ChainStatus), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync");
+        FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    }
+    if (!hs.failed) {
+        // The last solve, block by block, each block going down once solved
+        // (narrowed first when the panels are narrow, into a staging block
+        // whose previous contents have gone down). A failed chain writes
+        // nothing back: the panels keep Y.
+        for (int b = 0; b < nb; ++b) {
+            int64_t r0, r1;
+            B.rows(b, N, &r0, &r1);
+            FB_TRY(trsm_enqueue(Yz + r0, ldy, r1 - r0, k, U, k, trsm_ws, trsm_bytes, stream, st, GATE_HEALTHY));
+            if (narrow) {
+                if (b >= 2) FB_CUDA(cudaStreamWaitEvent(stream, sent[b - 2], 0), "cudaStreamWaitEvent");
+                FB_TRY(fb_convert_copy(stage[b & 1], FB_C64, sld, Yz + r0, FB_C128, ldy, r1 - r0, k, queue));
+            }
+            cudaEvent_t solved;
+            FB_TRY(events.make(&solved));
+            FB_CUDA(cudaEventRecord(solved, stream), "cudaEventRecord");
+            FB_CUDA(cudaStreamWaitEvent(down, solved, 0), "cudaStreamWaitEvent");
+            FB_TRY(copy_block(b, false, down));
+            FB_TRY(events.make(&sent[b]));
+            FB_CUDA(cudaEventRecord(sent[b], down), "cudaEventRecord");
+        }
+        FB_CUDA(cudaStreamWaitEvent(stream, sent[nb - 1], 0), "cudaStreamWaitEvent");
+    }
+    int blocks = (int)((int64_t)k * k + 255) / 256;
+    select_r_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<z64*>(R), ldr, Ra, Rb, k, st);
+    FB_LAUNCHED("select_r_kernel");
+    FB_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    int inf = 0;
+    const int status = fb_zcholqr2_query(st, &inf, passes, nullptr);
+    if (info) *info = inf;
+    return status;
 }
 
 }  // extern "C"

@@ -23,26 +23,30 @@ template <> __device__ __forceinline__ double convert_elem<double, float>(float 
 template <> __device__ __forceinline__ float convert_elem<float, double>(double s) { return __double2float_rn(s); }
 template <> __device__ __forceinline__ float convert_elem<float, float>(float s) { return s; }
 
+// Columns along y, rows along x (grid-strided), so no thread divides.
 template <typename D, typename S>
 __global__ void convert_kernel(D* __restrict__ dst, int64_t ldd, const S* __restrict__ src, int64_t lds,
                                int64_t rows, int64_t cols) {
-    const int64_t total = rows * cols;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        int64_t j = e / rows, i = e - j * rows;
-        dst[i + j * ldd] = convert_elem<D, S>(src[i + j * lds]);
+    for (int64_t j = blockIdx.y; j < cols; j += gridDim.y) {
+        D* dcol = dst + j * ldd;
+        const S* scol = src + j * lds;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride)
+            dcol[i] = convert_elem<D, S>(scol[i]);
     }
 }
 
 template <typename D, typename S>
 static int launch_convert(void* dst, int64_t ldd, const void* src, int64_t lds, int64_t rows, int64_t cols,
                           cudaStream_t stream) {
-    const int64_t total = rows * cols;
-    int64_t grid = (total + 255) / 256;
-    int64_t cap = (int64_t)sm_count() * 16;
-    if (grid > cap) grid = cap;
-    convert_kernel<D, S><<<(unsigned)grid, 256, 0, stream>>>(static_cast<D*>(dst), ldd, static_cast<const S*>(src),
-                                                             lds, rows, cols);
+    const int64_t gy = cols < 65535 ? cols : 65535;
+    int64_t gx = (rows + 255) / 256;
+    const int64_t want = (int64_t)sm_count() * 16;
+    const int64_t cap_x = (want + gy - 1) / gy;
+    if (gx > cap_x) gx = cap_x;
+    if (gx < 1) gx = 1;
+    convert_kernel<D, S><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, stream>>>(
+        static_cast<D*>(dst), ldd, static_cast<const S*>(src), lds, rows, cols);
     FB_LAUNCHED("convert_kernel");
     return FB_OK;
 }

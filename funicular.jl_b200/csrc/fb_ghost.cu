@@ -12,13 +12,21 @@
 //   real:    sqrt(-2 ln u1) cos 2 pi u2                              (N(0, 1))
 //
 // Philox4x32-10 is the counter-based generator of Salmon, Moraes, Dror and
-// Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC 2011); the
-// transform is Box and Muller (1958). ln, cos and sin are this file's own
-// (series about 1 and about 0 with 1/n and 1/n! coefficients, below), built
-// from + - * / sqrt and explicit fma only, and this file is compiled with
-// -fmad=false, so every entry rounds the same way on any IEEE machine: the
-// oracle's C restatement reproduces it bit for bit.
+// Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC 2011); its ten
+// round keys depend on the seed alone and are made on the host. The
+// transform is Box and Muller (1958). ln, cos and sin are this file's own,
+// table driven: ln m = ln(1/inv) + log1p(m inv - 1) with (inv, ln(1/inv)) of
+// the 8-bit bin m falls in and a degree-8 series for log1p on |r| < 2^-8;
+// cos and sin of 2 pi u by the angle sum from the centre of u's 8-bit bin,
+// the remaining angle below 2 pi 2^-9 taken to a^7 (sin) and a^6 (cos).
+// The tables (fb_ghost_tables.h) are generated to the nearest double from
+// 60-digit values. Only + - * sqrt and explicit fma are used, and this file
+// is compiled with -fmad=false, so every entry rounds the same way on any
+// IEEE machine: the oracle's C restatement reproduces it bit for bit.
 #include "fb_common.cuh"
+
+#define FB_GHOST_TABLE_QUALIFIER static __device__ const
+#include "fb_ghost_tables.h"
 
 namespace fb {
 namespace ghost {
@@ -26,83 +34,86 @@ namespace ghost {
 constexpr uint32_t PHILOX_M0 = 0xD2511F53u, PHILOX_M1 = 0xCD9E8D57u;
 constexpr uint32_t PHILOX_W0 = 0x9E3779B9u, PHILOX_W1 = 0xBB67AE85u;
 
-__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+// The ten round keys of a seed: key k_r = seed + r W (per 32-bit half).
+struct RoundKeys {
+    uint32_t k0[10], k1[10];
+};
+
+static RoundKeys round_keys(uint64_t seed) {
+    RoundKeys rk;
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        rk.k0[r] = k0;
+        rk.k1[r] = k1;
+        k0 += PHILOX_W0;
+        k1 += PHILOX_W1;
+    }
+    return rk;
+}
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], const RoundKeys& rk) {
 #pragma unroll
     for (int round = 0; round < 10; ++round) {
         const uint32_t lo0 = PHILOX_M0 * c[0], hi0 = __umulhi(PHILOX_M0, c[0]);
         const uint32_t lo1 = PHILOX_M1 * c[2], hi1 = __umulhi(PHILOX_M1, c[2]);
-        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        const uint32_t n0 = hi1 ^ c[1] ^ rk.k0[round], n2 = hi0 ^ c[3] ^ rk.k1[round];
         c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
-        k0 += PHILOX_W0; k1 += PHILOX_W1;
     }
 }
 
-// ln x for a positive normal x: x = 2^e m with m in (sqrt(1/2), sqrt(2)],
-// ln m = 2 atanh(s) with s = (m - 1) / (m + 1), |s| < 0.1716, summed to s^19.
-__device__ __forceinline__ double ln_pos(double x) {
+// The tables, staged in shared memory by each CTA.
+constexpr int LN_DOUBLES = 2 * FB_GHOST_LN_ENTRIES;
+constexpr int TRIG_DOUBLES = 2 * 256;
+
+// ln x for a positive normal x: x = 2^e m with m in (sqrt(1/2), sqrt(2)].
+__device__ __forceinline__ double ln_pos(double x, const double* __restrict__ lnt) {
     const long long bits = __double_as_longlong(x);
     int e = (int)((bits >> 52) & 0x7ff) - 1023;
     double m = __longlong_as_double((bits & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
     if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
-    const double f = m - 1.0;
-    const double s = f / (2.0 + f);
-    const double z = s * s;
-    double p = 1.0 / 19.0;
-    p = fma(p, z, 1.0 / 17.0);
-    p = fma(p, z, 1.0 / 15.0);
-    p = fma(p, z, 1.0 / 13.0);
-    p = fma(p, z, 1.0 / 11.0);
-    p = fma(p, z, 1.0 / 9.0);
-    p = fma(p, z, 1.0 / 7.0);
-    p = fma(p, z, 1.0 / 5.0);
-    p = fma(p, z, 1.0 / 3.0);
-    const double t = s + s;
-    const double lnm = fma(t * z, p, t);
-    return fma((double)e, 0.6931471805599453, lnm);
+    const int j = (int)((__double_as_longlong(m) >> 44) & 0xff);
+    const int idx = m >= 1.0 ? j : FB_GHOST_LN_UPPER_BINS + (j - FB_GHOST_LN_LOWER_FIRST);
+    const double inv = lnt[2 * idx], lninv = lnt[2 * idx + 1];
+    const double r = fma(m, inv, -1.0);
+    double p = -1.0 / 8.0;
+    p = fma(p, r, 1.0 / 7.0);
+    p = fma(p, r, -1.0 / 6.0);
+    p = fma(p, r, 1.0 / 5.0);
+    p = fma(p, r, -1.0 / 4.0);
+    p = fma(p, r, 1.0 / 3.0);
+    p = fma(p, r, -0.5);
+    const double l1p = fma(r * r, p, r);
+    const double hi = fma((double)e, FB_GHOST_LN2_HI, lninv);
+    const double lo = fma((double)e, FB_GHOST_LN2_LO, l1p);
+    return hi + lo;
 }
 
-// (cos, sin) of 2 pi u for u in [0, 1): quadrant q = round(4u), a = (4u - q) pi/2
-// in [-pi/4, pi/4], Taylor series to a^17 and a^18.
-__device__ __forceinline__ void cos_sin_2pi(double u, double& c, double& s) {
-    const double t = 4.0 * u;
-    const double qf = floor(t + 0.5);
-    const double r = t - qf;
-    const int q = ((int)qf) & 3;
-    const double a = r * 1.5707963267948966;
+// (cos, sin) of 2 pi u, u = b 2^-53 with b < 2^53: bin j = b >> 45 (centre
+// theta_j = 2 pi (j + 1/2) / 256), a = 2 pi (u - centre) in [-2 pi 2^-9,
+// 2 pi 2^-9).
+__device__ __forceinline__ void cos_sin_2pi(uint64_t b, const double* __restrict__ trig, double& c, double& s) {
+    const int j = (int)(b >> 45);
+    const long long f = (long long)(b & ((1ull << 45) - 1)) - (1ll << 44);
+    const double a = ((double)f * 0x1.0p-53) * FB_GHOST_TWO_PI;
     const double a2 = a * a;
-    double sp = 1.0 / 355687428096000.0;
-    sp = fma(sp, a2, -1.0 / 1307674368000.0);
-    sp = fma(sp, a2, 1.0 / 6227020800.0);
-    sp = fma(sp, a2, -1.0 / 39916800.0);
-    sp = fma(sp, a2, 1.0 / 362880.0);
-    sp = fma(sp, a2, -1.0 / 5040.0);
-    sp = fma(sp, a2, 1.0 / 120.0);
-    sp = fma(sp, a2, -1.0 / 6.0);
-    const double sa = fma(a * a2, sp, a);
-    double cp = -1.0 / 6402373705728000.0;
-    cp = fma(cp, a2, 1.0 / 20922789888000.0);
-    cp = fma(cp, a2, -1.0 / 87178291200.0);
-    cp = fma(cp, a2, 1.0 / 479001600.0);
-    cp = fma(cp, a2, -1.0 / 3628800.0);
-    cp = fma(cp, a2, 1.0 / 40320.0);
-    cp = fma(cp, a2, -1.0 / 720.0);
-    cp = fma(cp, a2, 1.0 / 24.0);
-    const double ca = fma(a2 * a2, cp, fma(a2, -0.5, 1.0));
-    switch (q) {
-        case 0: c = ca; s = sa; break;
-        case 1: c = -sa; s = ca; break;
-        case 2: c = -ca; s = -sa; break;
-        default: c = sa; s = -ca; break;
-    }
+    double ps = fma(a2, -1.0 / 5040.0, 1.0 / 120.0);
+    ps = fma(ps, a2, -1.0 / 6.0);
+    const double sa = fma(a * a2, ps, a);
+    double pc = fma(a2, -1.0 / 720.0, 1.0 / 24.0);
+    pc = fma(pc, a2, -0.5);
+    const double cm1 = a2 * pc;
+    const double C = trig[2 * j], S = trig[2 * j + 1];
+    c = C + fma(C, cm1, -(S * sa));
+    s = S + fma(S, cm1, C * sa);
 }
 
-__device__ __forceinline__ void uniforms(uint64_t seed, int64_t row, int64_t col, double& u1, double& u2) {
+__device__ __forceinline__ void uniforms(const RoundKeys& rk, int64_t row, int64_t col, double& u1, uint64_t& b2) {
     uint32_t c[4] = {(uint32_t)row, (uint32_t)((uint64_t)row >> 32), (uint32_t)col, (uint32_t)((uint64_t)col >> 32)};
-    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    philox4x32_10(c, rk);
     const uint64_t a = ((uint64_t)c[0] << 32) | c[1];
     const uint64_t b = ((uint64_t)c[2] << 32) | c[3];
     u1 = (double)((a >> 11) + 1) * 0x1.0p-53;
-    u2 = (double)(b >> 11) * 0x1.0p-53;
+    b2 = b >> 11;
 }
 
 template <typename D>
@@ -119,15 +130,21 @@ template <> __device__ __forceinline__ void store<float>(float* p, double re, do
 // which is what a narrowed host tier holds (src/ghosts.jl:109).
 template <typename D, bool COMPLEX>
 __global__ void __launch_bounds__(256) ghost_fill_kernel(D* __restrict__ dst, int64_t ld, int64_t rows, int64_t cols,
-                                                         int64_t row0, int64_t col0, uint64_t seed, int narrow) {
+                                                         int64_t row0, int64_t col0, const RoundKeys rk, int narrow) {
+    __shared__ double lnt[LN_DOUBLES];
+    __shared__ double trig[TRIG_DOUBLES];
+    for (int e = threadIdx.x; e < LN_DOUBLES; e += blockDim.x) lnt[e] = fb_ghost_ln_table[e];
+    for (int e = threadIdx.x; e < TRIG_DOUBLES; e += blockDim.x) trig[e] = fb_ghost_trig_table[e];
+    __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t j = blockIdx.y; j < cols; j += gridDim.y) {
         D* column = dst + j * ld;
         for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) {
-            double u1, u2, c, s;
-            uniforms(seed, row0 + i, col0 + j, u1, u2);
-            cos_sin_2pi(u2, c, s);
-            const double l = ln_pos(u1);
+            double u1, c, s;
+            uint64_t b2;
+            uniforms(rk, row0 + i, col0 + j, u1, b2);
+            cos_sin_2pi(b2, trig, c, s);
+            const double l = ln_pos(u1, lnt);
             double re, im;
             if (COMPLEX) {
                 const double rad = sqrt(-l);
@@ -157,7 +174,7 @@ static int launch_fill(void* dst, int64_t ld, int64_t rows, int64_t cols, int64_
     if (gx > cap_x) gx = cap_x;
     if (gx < 1) gx = 1;
     ghost_fill_kernel<D, COMPLEX><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, stream>>>(
-        static_cast<D*>(dst), ld, rows, cols, row0, col0, seed, narrow);
+        static_cast<D*>(dst), ld, rows, cols, row0, col0, round_keys(seed), narrow);
     FB_LAUNCHED("ghost_fill_kernel");
     return FB_OK;
 }

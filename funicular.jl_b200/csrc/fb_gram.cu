@@ -85,7 +85,7 @@ template <int PPW>
 __global__ void __launch_bounds__(PPW >= 8 ? 9 * 32 : PPW == 3 ? 13 * 32 : G_MAX_WARPS * 32, 1)
 gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  int64_t rows, GramShape sh, GramLaunch ln, z64* __restrict__ partial,
-                 const ChainStatus* st, int gate) {
+                 const ChainStatus* st, int gate, int chunk0) {
     if (gated_off(st, gate)) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // Aligned for the 128-byte swizzle by pointer arithmetic on the shared
@@ -110,7 +110,7 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         tj = blockIdx.x % sh.nt_b;
         tile_index = blockIdx.x;
     }
-    const int chunk = blockIdx.y;
+    const int chunk = chunk0 + (int)blockIdx.y;
     const int64_t row0 = (int64_t)chunk * sh.chunk_rows;
     const int64_t row_end = min(rows, row0 + sh.chunk_rows);
     const int64_t nstages = (row_end - row0 + GS_ROWS - 1) / GS_ROWS;
@@ -287,7 +287,9 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 acc[0][i][x][1] += acc[h][i][x][1];
             }
 
-    z64* out = partial + ((size_t)tile_index * sh.nchunks + chunk) * (G_TILE * G_TILE);
+    // A partial tile holds tw_a x tw_b entries, column-major: narrow tiles
+    // take only the scratch they fill.
+    z64* out = partial + ((size_t)tile_index * sh.nchunks + chunk) * (size_t)(sh.tw_a * sh.tw_b);
 #pragma unroll
     for (int i = 0; i < PPW; ++i) {
         if (!valid[i]) continue;
@@ -295,7 +297,7 @@ gram_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const int lj = bj[i] * 8 + 2 * (lane & 3) + c;
-            out[lj * G_TILE + li] = zmake(acc[0][i][0][c], dpair[i] ? 0.0 : acc[0][i][1][c]);
+            out[lj * sh.tw_a + li] = zmake(acc[0][i][0][c], dpair[i] ? 0.0 : acc[0][i][1][c]);
         }
     }
 }
@@ -318,15 +320,17 @@ __global__ void gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int kA, int
     int tile;
     if (sh.hermitian) tile = (ti == tj) ? ti : off_tile_index(sh.nt_a, ti, tj);
     else tile = ti * sh.nt_b + tj;
-    const z64* src = partial + (size_t)tile * sh.nchunks * (G_TILE * G_TILE) + lj * G_TILE + li;
+    const size_t tile_entries = (size_t)(sh.tw_a * sh.tw_b);
+    const z64* src = partial + (size_t)tile * sh.nchunks * tile_entries + lj * sh.tw_a + li;
     // A diagonal 8 x 8 block of a folded tile holds S = Re + Im: Re and Im
-    // come back as the symmetric and antisymmetric parts of S.
+    // come back as the symmetric and antisymmetric parts of S. Folded tiles
+    // are square (tw_a == tw_b).
     const bool sblock = sh.sdiag && ti == tj && (li >> 3) == (lj >> 3);
-    const z64* srcT = partial + (size_t)tile * sh.nchunks * (G_TILE * G_TILE) + li * G_TILE + lj;
+    const z64* srcT = partial + (size_t)tile * sh.nchunks * tile_entries + li * sh.tw_a + lj;
     z64 s = zmake(0.0, 0.0);
     for (int c = lane; c < sh.nchunks; c += 32) {
-        z64 v = src[(size_t)c * (G_TILE * G_TILE)];
-        if (sblock) v.y = srcT[(size_t)c * (G_TILE * G_TILE)].x;
+        z64 v = src[(size_t)c * tile_entries];
+        if (sblock) v.y = srcT[(size_t)c * tile_entries].x;
         s.x += v.x;
         s.y += v.y;
     }
@@ -500,51 +504,76 @@ static int gram_ctas_per_sm(int64_t rows, int kA, int kB, bool hermitian) {
 
 template <int PPW>
 static int launch_gram_dmma(const CUtensorMap& ma, const CUtensorMap& mb, int64_t rows, const GramShape& sh,
-                            const GramLaunch& ln, z64* partial, cudaStream_t stream, const ChainStatus* st, int gate) {
+                            const GramLaunch& ln, z64* partial, cudaStream_t stream, const ChainStatus* st, int gate,
+                            int chunk0, int chunk1) {
     FB_TRY(set_gram_attr<PPW>(ln.smem));
-    dim3 grid(ln.ntiles, sh.nchunks);
-    gram_dmma_kernel<PPW><<<grid, (ln.consumers + 1) * 32, ln.smem, stream>>>(ma, mb, rows, sh, ln, partial, st, gate);
+    dim3 grid(ln.ntiles, chunk1 - chunk0);
+    gram_dmma_kernel<PPW><<<grid, (ln.consumers + 1) * 32, ln.smem, stream>>>(ma, mb, rows, sh, ln, partial, st, gate,
+                                                                              chunk0);
     FB_LAUNCHED("gram_dmma_kernel");
     return FB_OK;
 }
 
 static size_t gram_workspace_bytes(const GramShape& sh) {
-    return (size_t)sh.ntiles * (size_t)(sh.nchunks > 0 ? sh.nchunks : 1) * G_TILE * G_TILE * sizeof(z64);
+    return (size_t)sh.ntiles * (size_t)(sh.nchunks > 0 ? sh.nchunks : 1) * (size_t)(sh.tw_a * sh.tw_b) * sizeof(z64);
 }
 
-// Shared by fb_zgram and the orthonormalization chain.
-int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, int64_t ldb,
-                 int64_t rows, int kA, int kB, z64 alpha, z64 beta, bool hermitian,
-                 void* workspace, size_t workspace_bytes, cudaStream_t stream,
-                 const ChainStatus* st, int gate) {
-    GramShape sh = gram_shape(rows, kA, kB, hermitian ? 1 : 0, gram_ctas_per_sm(rows, kA, kB, hermitian));
+static GramShape gram_plan(int64_t rows, int kA, int kB, bool hermitian) {
+    return gram_shape(rows, kA, kB, hermitian ? 1 : 0, gram_ctas_per_sm(rows, kA, kB, hermitian));
+}
+
+// The row chunks of a Gram: chunk c covers rows [c chunk_rows, (c + 1)
+// chunk_rows). Each chunk's partial tiles depend on its rows alone, so the
+// partials of a chunk range can be computed as soon as those rows are in
+// place (a pipelined upload), with the same bits as one launch over all.
+void gram_chunks(int64_t rows, int kA, int kB, bool hermitian, int64_t* chunk_rows, int* nchunks) {
+    const GramShape sh = gram_plan(rows, kA, kB, hermitian);
+    *chunk_rows = sh.chunk_rows;
+    *nchunks = sh.nchunks;
+}
+
+// The partial tiles of chunks [chunk0, chunk1).
+int gram_partials_enqueue(const z64* A, int64_t lda, const z64* B, int64_t ldb, int64_t rows, int kA, int kB,
+                          bool hermitian, void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                          const ChainStatus* st, int gate, int chunk0, int chunk1) {
+    GramShape sh = gram_plan(rows, kA, kB, hermitian);
     size_t need = gram_workspace_bytes(sh);
     if (workspace_bytes < need || workspace == nullptr) {
         set_error(FB_ENOMEM, "gram: workspace of %zu bytes is smaller than the %zu bytes this shape needs",
                   workspace_bytes, need);
         return FB_ENOMEM;
     }
+    if (chunk0 < 0) chunk0 = 0;
+    if (chunk1 > sh.nchunks) chunk1 = sh.nchunks;
+    if (chunk0 >= chunk1) return FB_OK;
     z64* partial = static_cast<z64*>(workspace);
-    if (sh.nchunks > 0) {
-        CUtensorMap ma, mb;
-        FB_TRY(encode_panel_map(&ma, A, rows, kA, lda, sh.tw_a));
-        FB_TRY(encode_panel_map(&mb, B, rows, kB, ldb, sh.tw_b));
-        if (hermitian) sh.sdiag = gram_launch(sh, true).sdiag;
-        const bool launches[2] = {hermitian, !hermitian || sh.nt_a > 1};
-        for (int d = 0; d < 2; ++d) {
-            if (!launches[d]) continue;
-            GramLaunch ln = gram_launch(sh, d == 0);
-            if (ln.ntiles == 0) continue;
-            int status;
-            switch (ln.ppw) {
-                case 2: status = launch_gram_dmma<2>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
-                case 3: status = launch_gram_dmma<3>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
-                case 4: status = launch_gram_dmma<4>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
-                default: status = launch_gram_dmma<8>(ma, mb, rows, sh, ln, partial, stream, st, gate); break;
-            }
-            FB_TRY(status);
+    CUtensorMap ma, mb;
+    FB_TRY(encode_panel_map(&ma, A, rows, kA, lda, sh.tw_a));
+    FB_TRY(encode_panel_map(&mb, B, rows, kB, ldb, sh.tw_b));
+    if (hermitian) sh.sdiag = gram_launch(sh, true).sdiag;
+    const bool launches[2] = {hermitian, !hermitian || sh.nt_a > 1};
+    for (int d = 0; d < 2; ++d) {
+        if (!launches[d]) continue;
+        GramLaunch ln = gram_launch(sh, d == 0);
+        if (ln.ntiles == 0) continue;
+        int status;
+        switch (ln.ppw) {
+            case 2: status = launch_gram_dmma<2>(ma, mb, rows, sh, ln, partial, stream, st, gate, chunk0, chunk1); break;
+            case 3: status = launch_gram_dmma<3>(ma, mb, rows, sh, ln, partial, stream, st, gate, chunk0, chunk1); break;
+            case 4: status = launch_gram_dmma<4>(ma, mb, rows, sh, ln, partial, stream, st, gate, chunk0, chunk1); break;
+            default: status = launch_gram_dmma<8>(ma, mb, rows, sh, ln, partial, stream, st, gate, chunk0, chunk1); break;
         }
+        FB_TRY(status);
     }
+    return FB_OK;
+}
+
+// C <- alpha (sum of the partial tiles of every chunk) + beta C.
+int gram_reduce_enqueue(z64* C, int64_t ldc, int64_t rows, int kA, int kB, bool hermitian, z64 alpha, z64 beta,
+                        void* workspace, cudaStream_t stream, const ChainStatus* st, int gate) {
+    GramShape sh = gram_plan(rows, kA, kB, hermitian);
+    if (hermitian && sh.nchunks > 0) sh.sdiag = gram_launch(sh, true).sdiag;
+    z64* partial = static_cast<z64*>(workspace);
     int64_t entries = (int64_t)kA * kB;
     int64_t threads = entries * 32;
     int block = 256;
@@ -554,8 +583,25 @@ int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, i
     return FB_OK;
 }
 
+// Shared by fb_zgram and the orthonormalization chain.
+int gram_enqueue(z64* C, int64_t ldc, const z64* A, int64_t lda, const z64* B, int64_t ldb,
+                 int64_t rows, int kA, int kB, z64 alpha, z64 beta, bool hermitian,
+                 void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                 const ChainStatus* st, int gate) {
+    const GramShape sh = gram_plan(rows, kA, kB, hermitian);
+    const size_t need = gram_workspace_bytes(sh);
+    if (workspace_bytes < need || workspace == nullptr) {
+        set_error(FB_ENOMEM, "gram: workspace of %zu bytes is smaller than the %zu bytes this shape needs",
+                  workspace_bytes, need);
+        return FB_ENOMEM;
+    }
+    FB_TRY(gram_partials_enqueue(A, lda, B, ldb, rows, kA, kB, hermitian, workspace, workspace_bytes, stream, st,
+                                 gate, 0, sh.nchunks));
+    return gram_reduce_enqueue(C, ldc, rows, kA, kB, hermitian, alpha, beta, workspace, stream, st, gate);
+}
+
 size_t gram_workspace_size(int64_t rows, int kA, int kB, bool hermitian) {
-    return gram_workspace_bytes(gram_shape(rows, kA, kB, hermitian ? 1 : 0, gram_ctas_per_sm(rows, kA, kB, hermitian)));
+    return gram_workspace_bytes(gram_plan(rows, kA, kB, hermitian));
 }
 
 // Scratch for fb_zgram_static, the entry point for callers that cannot

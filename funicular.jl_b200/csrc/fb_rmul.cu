@@ -22,7 +22,8 @@ __host__ __device__ constexpr int rm_split(int ntn) { return ntn >= 8 ? 2 : 1; }
 template <int NTK, int NTN>
 __global__ void __launch_bounds__(RM_THREADS, 1)
 rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2, int64_t rows,
-                 int K, int n, const double* __restrict__ gdense, const double* __restrict__ glower, z64 beta,
+                 int K, int n, const double* __restrict__ gdense, const double* __restrict__ glower,
+                 const z64* __restrict__ Cm, int64_t ldcm, z64 beta,
                  int use_beta, int zero, int inplace, const ChainStatus* st, int gate) {
     if (gated_off(st, gate)) return;
     constexpr int NS = 2 * NTK;               // k-steps
@@ -36,7 +37,16 @@ rmul_dmma_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
     double* fd = reinterpret_cast<double*>(smem_raw);
     double* fl = fd + dense_frag_doubles(NTK, NTN);
     const bool lower = SQUARE && A1 != nullptr;
-    {
+    if (gdense == nullptr) {
+        // The factor given as a K x n matrix (the plain product A2 C): every
+        // CTA lays out the fragments of the whole template-sized factor
+        // itself, zero past K and n.
+        for (int e = threadIdx.x; e < dense_frag_doubles(NTK, NTN); e += blockDim.x) {
+            const int l = e & 31, q = e >> 5;
+            const int s = q / NTN, t = q - s * NTN;
+            fd[e] = frag_entry(Cm, ldcm, K, n, s, t, l, 1.0);
+        }
+    } else {
         const double2* s2 = reinterpret_cast<const double2*>(gdense);
         double2* d2 = reinterpret_cast<double2*>(fd);
         for (int e = threadIdx.x; e < dense_frag_doubles(NTK, NTN) / 2; e += blockDim.x) d2[e] = s2[e];
@@ -149,7 +159,8 @@ rmul_rows_kernel(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* __
 template <int NTK, int NTN>
 static int launch_rmul_dmma(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2,
                             int64_t rows, int K, int n, const double* fdense, const double* flower, z64 beta,
-                            int use_beta, cudaStream_t stream, const ChainStatus* st, int gate) {
+                            int use_beta, cudaStream_t stream, const ChainStatus* st, int gate,
+                            const z64* Cm = nullptr, int64_t ldcm = 0) {
     const bool lower = NTK == NTN && A1 != nullptr;
     const size_t smem = (size_t)(dense_frag_doubles(NTK, NTN) + (lower ? lower_frag_doubles(NTN) : 0)) * sizeof(double);
     FB_CUDA(cudaFuncSetAttribute(rmul_dmma_kernel<NTK, NTN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -166,9 +177,45 @@ static int launch_rmul_dmma(z64* D, int64_t ldd, const z64* A1, int64_t lda1, co
     if (grid < 1) grid = 1;
     const int inplace = (D == A1 || D == A2) ? 1 : 0;
     rmul_dmma_kernel<NTK, NTN><<<(unsigned)grid, RM_THREADS, smem, stream>>>(
-        D, ldd, lower ? A1 : nullptr, lda1, A2, lda2, rows, K, n, fdense, flower, beta, use_beta, 0, inplace, st, gate);
+        D, ldd, lower ? A1 : nullptr, lda1, A2, lda2, rows, K, n, fdense, flower, Cm, ldcm, beta, use_beta, 0, inplace,
+        st, gate);
     FB_LAUNCHED("rmul_dmma_kernel");
     return FB_OK;
+}
+
+// D <- beta D (when use_beta) + A C for a K x n factor C given as a matrix,
+// K, n <= 64, on the tensor cores. The template is the smallest one that
+// holds the factor: square when K and n take the same number of 4-column
+// tiles or K takes fewer (K padded with zeros), 64 rows of K otherwise.
+int rmul_matrix_enqueue(z64* D, int64_t ldd, const z64* A, int64_t lda, int64_t rows, int K, int n, const z64* C,
+                        int64_t ldc, z64 beta, int use_beta, cudaStream_t stream) {
+    if (rows == 0 || n == 0) return FB_OK;
+    if (K < 1 || K > RM_KMAX || n > RM_KMAX) {
+        set_error(FB_EINVAL, "rmul: a %d x %d factor is past the 64 x 64 the tensor-core product takes", K, n);
+        return FB_EINVAL;
+    }
+    const int ntk = (K + 3) / 4, ntn = (n + 3) / 4;
+    if (ntk <= ntn) {
+        switch (ntn) {
+#define FB_RM_MSQ(t) \
+    case t: return launch_rmul_dmma<t, t>(D, ldd, nullptr, 0, A, lda, rows, K, n, nullptr, nullptr, beta, use_beta, stream, nullptr, GATE_ALWAYS, C, ldc);
+            FB_RM_MSQ(1) FB_RM_MSQ(2) FB_RM_MSQ(3) FB_RM_MSQ(4) FB_RM_MSQ(5) FB_RM_MSQ(6) FB_RM_MSQ(7) FB_RM_MSQ(8)
+            FB_RM_MSQ(9) FB_RM_MSQ(10) FB_RM_MSQ(11) FB_RM_MSQ(12) FB_RM_MSQ(13) FB_RM_MSQ(14) FB_RM_MSQ(15)
+            FB_RM_MSQ(16)
+#undef FB_RM_MSQ
+        }
+    } else {
+        switch (ntn) {
+#define FB_RM_MWIDE(t) \
+    case t: return launch_rmul_dmma<16, t>(D, ldd, nullptr, 0, A, lda, rows, K, n, nullptr, nullptr, beta, use_beta, stream, nullptr, GATE_ALWAYS, C, ldc);
+            FB_RM_MWIDE(1) FB_RM_MWIDE(2) FB_RM_MWIDE(3) FB_RM_MWIDE(4) FB_RM_MWIDE(5) FB_RM_MWIDE(6) FB_RM_MWIDE(7)
+            FB_RM_MWIDE(8) FB_RM_MWIDE(9) FB_RM_MWIDE(10) FB_RM_MWIDE(11) FB_RM_MWIDE(12) FB_RM_MWIDE(13)
+            FB_RM_MWIDE(14) FB_RM_MWIDE(15)
+#undef FB_RM_MWIDE
+        }
+    }
+    set_error(FB_EINVAL, "rmul: no template for a %d x %d factor", K, n);
+    return FB_EINVAL;
 }
 
 int rmul_enqueue(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2, int64_t lda2, int64_t rows,

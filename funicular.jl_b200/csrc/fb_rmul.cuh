@@ -73,4 +73,10 @@ int rmul_enqueue(z64* D, int64_t ldd, const z64* A1, int64_t lda1, const z64* A2
                  int K, int n, const z64* L, int64_t ldl, const z64* C, int64_t ldc, const double* fdense,
                  const double* flower, z64 beta, int use_beta, cudaStream_t stream, const ChainStatus* st, int gate);
 
+// D <- beta D (when use_beta) + A C, A rows x K, C a K x n device matrix
+// (leading dimension ldc), K and n at most 64, on the tensor cores: each CTA
+// lays out C's fragments in shared memory itself. D must not overlap A.
+int rmul_matrix_enqueue(z64* D, int64_t ldd, const z64* A, int64_t lda, int64_t rows, int K, int n, const z64* C,
+                        int64_t ldc, z64 beta, int use_beta, cudaStream_t stream);
+
 }  // namespace fb

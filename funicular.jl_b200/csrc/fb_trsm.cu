@@ -73,57 +73,6 @@ int trsm_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, int64_t
     return FB_OK;
 }
 
-// dst <- A C. A thread owns a row and produces its outputs TB columns at a
-// time: a loop over the s columns of A (read from the row) accumulates
-// the block against row i of C, staged in shared memory.
-constexpr int TB = 16;
-
-__global__ void __launch_bounds__(128)
-gemm_right_kernel(z64* __restrict__ D, int64_t ldd, const z64* __restrict__ A, int64_t lda,
-                  int64_t rows, int s, const z64* __restrict__ C, int64_t ldc, int r) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    z64* Cs = reinterpret_cast<z64*>(smem_raw);  // s x rp, row-major, zero past r
-    const int rp = (r + TB - 1) / TB * TB;
-    for (int e = threadIdx.x; e < s * rp; e += blockDim.x) {
-        int i = e / rp, j = e - i * rp;
-        Cs[e] = (j < r) ? C[i + (int64_t)j * ldc] : zmake(0.0, 0.0);
-    }
-    __syncthreads();
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += stride) {
-        const z64* arow = A + row;
-        for (int j0 = 0; j0 < rp; j0 += TB) {
-            z64 acc[TB];
-#pragma unroll
-            for (int c = 0; c < TB; ++c) acc[c] = zmake(0.0, 0.0);
-#pragma unroll 2
-            for (int i = 0; i < s; ++i) {
-                const z64 a = arow[(int64_t)i * lda];
-                const z64* Ci = Cs + i * rp + j0;
-#pragma unroll
-                for (int c = 0; c < TB; ++c) zmac(acc[c], a, Ci[c]);
-            }
-#pragma unroll
-            for (int c = 0; c < TB; ++c)
-                if (j0 + c < r) D[row + (int64_t)(j0 + c) * ldd] = acc[c];
-        }
-    }
-}
-
-// Factors too large for shared memory: the same loop, C through the
-// read-only cache.
-__global__ void gemm_right_generic_kernel(z64* __restrict__ D, int64_t ldd, const z64* __restrict__ A, int64_t lda,
-                                          int64_t rows, int s, const z64* __restrict__ C, int64_t ldc, int r) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += stride) {
-        for (int j = 0; j < r; ++j) {
-            z64 acc = zmake(0.0, 0.0);
-            for (int i = 0; i < s; ++i) zmac(acc, A[row + (int64_t)i * lda], __ldg(C + i + (int64_t)j * ldc));
-            D[row + (int64_t)j * ldd] = acc;
-        }
-    }
-}
-
 }  // namespace fb
 
 using namespace fb;
@@ -181,27 +130,18 @@ int fb_zgemm_right(fb_z128* dst, int64_t ldd, const fb_z128* A, int64_t lda, int
         FB_CUDA(cudaMemset2DAsync(D, ldd * sizeof(z64), 0, rows * sizeof(z64), r, stream), "cudaMemset2DAsync");
         return FB_OK;
     }
-    const int threads = 128;
-    const int rp = (r + TB - 1) / TB * TB;
-    size_t smem = (size_t)s * rp * sizeof(z64);
-    int64_t need = (rows + threads - 1) / threads;
-    if (smem <= 227 * 1024) {
-        FB_CUDA(cudaFuncSetAttribute(gemm_right_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                "cudaFuncSetAttribute(gemm_right_kernel)");
-        int per_sm = 0;
-        FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gemm_right_kernel, threads, smem),
-                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        if (per_sm < 1) per_sm = 1;
-        int64_t grid = (int64_t)sm_count() * per_sm;
-        if (grid > need) grid = need;
-        gemm_right_kernel<<<(unsigned)grid, threads, smem, stream>>>(D, ldd, Az, lda, rows, s, Cz, ldc, r);
-        FB_LAUNCHED("gemm_right_kernel");
-        return FB_OK;
+    // On the FP64 tensor cores (the right product of fb_rmul.cu), in blocks of
+    // at most 64 x 64 of the factor: output columns 64 at a time, and the s
+    // columns of A 64 at a time, each block accumulated onto the output (the
+    // first overwrites it, NaN included).
+    for (int j0 = 0; j0 < r; j0 += RM_KMAX) {
+        const int nb = r - j0 < RM_KMAX ? r - j0 : RM_KMAX;
+        for (int i0 = 0; i0 < s; i0 += RM_KMAX) {
+            const int kb = s - i0 < RM_KMAX ? s - i0 : RM_KMAX;
+            FB_TRY(rmul_matrix_enqueue(D + (int64_t)j0 * ldd, ldd, Az + (int64_t)i0 * lda, lda, rows, kb, nb,
+                                       Cz + i0 + (int64_t)j0 * ldc, ldc, zmake(1.0, 0.0), i0 > 0 ? 1 : 0, stream));
+        }
     }
-    int64_t grid = (int64_t)sm_count() * 8;
-    if (grid > need) grid = need;
-    gemm_right_generic_kernel<<<(unsigned)grid, threads, 0, stream>>>(D, ldd, Az, lda, rows, s, Cz, ldc, r);
-    FB_LAUNCHED("gemm_right_generic_kernel");
     return FB_OK;
 }
 

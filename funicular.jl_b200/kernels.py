@@ -217,6 +217,58 @@ def cholqr2_resident(backend, Y: DeviceMatrix, R: DeviceMatrix, wait: bool = Tru
     return passes.value, tuple(shifts)
 
 
+def cholqr2_staged(backend, panels, D: DeviceMatrix, R: DeviceMatrix, unit_roundoff: float = 0.0):
+    """cholqr2! end to end on a matrix held in page-locked host panels (a
+    list of N x w_p column-major arrays in column order, all complex128 or
+    all complex64 for a narrowed tier, e.g. a PanelMatrix's host storage): the
+    panels go up in row blocks while the first Gram consumes them (widened on
+    the device), the FP64 chain runs on the device (D is the N x k complex128
+    staging copy), and the last solve's row blocks come back into the panels
+    as they are solved (narrowed on the device). unit_roundoff > 0 runs the
+    shifted CholeskyQR3 instead. R (device) is written. Returns (passes,
+    shifts); raises NotPositiveDefinite, leaving the panels as they were,
+    when a Gram matrix stays indefinite. For complex128 panels, the same bits
+    as cholqr2_resident on D."""
+    _need_complex128(D, R)
+    N, k = D.shape
+    if R.shape != (k, k):
+        raise DimensionMismatch(f"cholqr2! of an {N}x{k} matrix writes a {k}x{k} R, got {R.shape}")
+    arrays = [np.asarray(a) for a in panels]
+    host_dtype = arrays[0].dtype if arrays else np.dtype(np.complex128)
+    if host_dtype not in (np.complex128, np.complex64):
+        raise ArgumentError(f"host panels are ComplexF64 or ComplexF32, got {host_dtype}")
+    for a in arrays:
+        if a.dtype != host_dtype or a.ndim != 2 or a.shape[0] != N or not a.flags.f_contiguous:
+            raise DimensionMismatch(f"a host panel of an {N}-row matrix must be N x w column major of one eltype, "
+                                    f"got {a.shape} {a.dtype}")
+    if sum(a.shape[1] for a in arrays) != k:
+        raise DimensionMismatch(f"the panels hold {sum(a.shape[1] for a in arrays)} columns, the matrix {k}")
+    host_type = _lib.FB_C128 if host_dtype == np.complex128 else _lib.FB_C64
+    n = len(arrays)
+    ptrs = (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrays])
+    lds = (ctypes.c_int64 * n)(*[N for _ in arrays])
+    cols = (ctypes.c_int * n)(*[a.shape[1] for a in arrays])
+    need = ctypes.c_size_t(0)
+    call("fb_zcholqr2_staged_workspace_size", ctypes.c_int64(N), k, host_type, ctypes.byref(need))
+    ws, ws_bytes = backend.workspace(need.value)
+    lib = _lib.load()
+    info = ctypes.c_int(0)
+    passes = ctypes.c_int(0)
+    try:
+        status = lib.fb_zcholqr2_staged(ptrs, host_type, lds, cols, n, _vp(D.ptr), D.ld, N, k, _vp(R.ptr), R.ld,
+                                        float(unit_roundoff), ctypes.byref(info), ctypes.byref(passes), _vp(ws),
+                                        ws_bytes, backend.queue_handle())
+        shifts = (ctypes.c_double * 3)()
+        if status == _lib.FB_OK:
+            status = lib.fb_zcholqr2_query(_vp(ws), None, None, shifts)
+    finally:
+        backend.workspace_release()
+    if status == _lib.FB_ENOTSPD:
+        raise NotPositiveDefinite(_lib.last_error())
+    _lib.check(status, "cholqr2!")
+    return passes.value, tuple(shifts)
+
+
 def ghost_fill(backend, dst: DeviceMatrix, row0: int, col0: int, seed: int, value_dtype) -> DeviceMatrix:
     """The device fill behind GhostPanels (generate_panel!, src/ghosts.jl:97-103,
     plus the upload that followed it): dst <- the ghost block whose top left

@@ -298,6 +298,24 @@ def cholqr2_resident(Y: PanelMatrix, form: str = "fp64", unit_roundoff=None) -> 
         for p in Y.panels:
             if p.hold is not None:
                 backend.wait_event(q, p.hold)
+        from .panels import host_storage_eltype
+        S = np.dtype(host_storage_eltype(plan, Y.dtype))
+        if form in ("fp64", "shifted3") and Y.dtype == np.complex128 and S in (np.complex128, np.complex64):
+            # The staged form: the upload overlaps the first Gram and the
+            # download the last solve, narrow tiers widened and narrowed on
+            # the device block by block.
+            u = 0.0 if form == "fp64" else (unit_roundoff if unit_roundoff is not None
+                                            else kernels.UNIT_ROUNDOFF[np.dtype(np.complex128)])
+            backend.submit(q, lambda: kernels.cholqr2_staged(backend, [p.storage() for p in Y.panels], D, Rd,
+                                                             unit_roundoff=u))
+            R = np.empty((Y.k, Y.k), dtype=Y.dtype, order="F")
+            backend.d2h(R, Rd, queue=q)
+            backend.sync_queue(q)
+            for p in Y.panels:
+                p.hold = None
+                p.dirty = True
+                p.epoch += 1
+            return R
         to_device(Y, D, q)
         # Waits for the chain and raises NotPositiveDefinite if it stopped.
         extra = {} if unit_roundoff is None else {"unit_roundoff": unit_roundoff}
@@ -353,12 +371,96 @@ def cholqr3(Y: PanelMatrix, *, nbuffers=None, resident=None, unit_roundoff=None)
 
 # ---- project (src/panelblas.jl:268-301) ---------------------------------------
 
-def project(Q: PanelMatrix, G: DeviceOperator, *, nbuffers=None) -> np.ndarray:
-    """project(Q, G; nbuffers): Q^H (G Q) block column by block column, p(p+1)
-    steps, one extra N x w image buffer."""
+PROJECT_SCHEDULES = ("resident", "two-sweep", "nested")
+
+
+def project_schedule(Q: PanelMatrix) -> str:
+    """The cheapest project schedule the plan affords: 'resident' when Q and
+    G Q fit the device budget together (Q crosses the bus once), 'two-sweep'
+    when the host has room for an N x k matrix Z (panelmul!(Z, G, Q) then
+    gram(Q, Z), src/panelblas.jl:250-261: three crossings of the matrix),
+    else the reference's nested schedule (p (p + 1) panel uploads)."""
+    from .panels import host_storage_eltype
+    from .plan import host_bytes_in_use
+    nbytes = Q.N * Q.k * Q.dtype.itemsize
+    pool = Q.plan.devicepool
+    if pool.allocated + 2 * nbytes + Q.k * Q.k * Q.dtype.itemsize <= pool.budget:
+        return "resident"
+    host_bytes = Q.N * Q.k * np.dtype(host_storage_eltype(Q.plan, Q.dtype)).itemsize
+    if Q.plan.hostpool.budget - host_bytes_in_use(Q.plan) >= host_bytes + 64 * Q.npanels():
+        return "two-sweep"
+    return "nested"
+
+
+def project(Q: PanelMatrix, G: DeviceOperator, *, nbuffers=None, schedule=None) -> np.ndarray:
+    """project(Q, G; nbuffers) (src/panelblas.jl:268-301): S = Q^H (G Q).
+    schedule None takes project_schedule(Q); 'nested' is the reference's
+    block-column schedule, 'two-sweep' its documented replacement when a
+    second N x k matrix fits on the host (src/panelblas.jl:258-260,
+    docs/src/porting.md:42-44), 'resident' the device-resident form: Q up
+    once, G applied to all of Q, one cross Gram on the device."""
+    assert_square_operator(G, Q.N)
+    schedule = project_schedule(Q) if schedule is None else schedule
+    if schedule not in PROJECT_SCHEDULES:
+        raise ArgumentError(f"project schedule is one of {PROJECT_SCHEDULES}, got {schedule!r}")
+    if schedule == "resident":
+        return project_resident(Q, G)
+    if schedule == "two-sweep":
+        try:
+            Z = PanelMatrix.undef(Q.dtype, Q.N, Q.k, plan=Q.plan, w=Q.w)
+        except ArgumentError:
+            # The host tier could not hold Z after all (its blocks are cut
+            # for other sizes): the nested schedule needs no second matrix.
+            return project_nested(Q, G, nbuffers=nbuffers)
+        return project_two_sweep(Q, G, Z, nbuffers=nbuffers)
+    return project_nested(Q, G, nbuffers=nbuffers)
+
+
+def project_resident(Q: PanelMatrix, G: DeviceOperator) -> np.ndarray:
+    """Q^H (G Q) with Q and G Q resident: every panel goes up once (a ghost is
+    generated on the device), the operator is applied to the whole N x k
+    matrix, and one cross Gram forms S."""
     plan = Q.plan
     backend = plan.backend
-    assert_square_operator(G, Q.N)
+    D, Z = checkout_device_buffers(plan, Q.dtype, (Q.N, Q.k), 2)
+    (acc,) = checkout_device_buffers(plan, Q.dtype, (Q.k, Q.k), 1)
+    try:
+        q = backend.make_queue()
+        for p in Q.panels:
+            if p.hold is not None:
+                backend.wait_event(q, p.hold)
+        to_device(Q, D, q)
+
+        def work():
+            apply_operator(backend, Z, G, D)
+            kernels.gram_accumulate(backend, acc, D, Z, 1.0, 0.0)
+
+        backend.submit(q, work)
+        S = np.empty((Q.k, Q.k), dtype=Q.dtype, order="F")
+        backend.d2h(S, acc, queue=q)
+        backend.sync_queue(q)
+        return S
+    finally:
+        checkin_device_buffers(plan, [D, Z, acc])
+
+
+def project_two_sweep(Q: PanelMatrix, G: DeviceOperator, Z: PanelMatrix, *, nbuffers=None) -> np.ndarray:
+    """panelmul!(Z, G, Q) into the host matrix Z (cut like Q), then
+    gram(Q, Z): two sweeps (src/panelblas.jl:258-260); Z is given back
+    afterwards."""
+    from .panels import free
+    try:
+        panelmul(Z, G, Q, nbuffers=nbuffers)
+        return gram(Q, Z, nbuffers=nbuffers)
+    finally:
+        free(Z)
+
+
+def project_nested(Q: PanelMatrix, G: DeviceOperator, *, nbuffers=None) -> np.ndarray:
+    """The reference's schedule: Q^H (G Q) block column by block column,
+    p(p+1) steps, one extra N x w image buffer."""
+    plan = Q.plan
+    backend = plan.backend
     p = Q.npanels()
     panels, labels = [], []
     for j in range(p):

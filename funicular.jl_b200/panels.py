@@ -116,8 +116,20 @@ class PanelMatrix:
                 "its own instead")
 
     def copy_from(self, A) -> "PanelMatrix":
-        """copyto!(pm, A) for a dense host matrix (src/panels.jl:242-270)."""
+        """copyto!(pm, A) for a dense host matrix (src/panels.jl:242-270), or
+        copyto!(dest, src) for a panel matrix source of the same N and k and
+        any panel width (src/panels.jl:317-320), a ghost included."""
         self.assert_writable()
+        if isinstance(A, PanelMatrix):
+            if A is self:
+                raise ArgumentError("copycols! cannot copy a panel matrix into itself, since the two ranges may "
+                                    "overlap and a column would then be read after it had already been "
+                                    "overwritten. Copy into a matrix of its own and copy that back")
+            if (A.N, A.k) != (self.N, self.k):
+                raise DimensionMismatch(f"the source is {A.N}×{A.k} and the destination is {self.N}×{self.k}, and "
+                                        "a whole-matrix copy moves column j of the source into column j of the "
+                                        "destination. Use copycols! to copy part of one matrix into part of another")
+            A = A.to_array()
         A = np.asarray(A)
         if A.shape != self.shape:
             raise DimensionMismatch(f"cannot copy a {A.shape} matrix into a {self.shape} panel matrix")

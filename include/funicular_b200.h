@@ -156,13 +156,16 @@ int fb_zgram(fb_z128* C, int64_t ldc,
  * into the library: 32 MiB, held on every GPU that loads the library until
  * the process exits. Shapes whose scratch would not fit in it
  * (fb_zgram_workspace_size above 32 MiB, which takes many 64 x 64 output
- * tiles: every Gram of at most 128 columns fits) are refused with FB_ENOMEM
- * before anything is enqueued. The first call on each device looks up the array's device
- * address; make it before any stream capture begins. All calls share the one
- * array: two calls whose work can overlap on the GPU (different queues with no
- * event ordering them) race on it, while calls on one queue are safe. Each
- * call writes every part of the array it reads, so nothing has to be cleared
- * between calls. The call allocates nothing. */
+ * tiles: on a 148-SM B200 every Gram of at most 128 columns a side fits,
+ * whatever the row count) are refused with FB_ENOMEM before anything is
+ * enqueued. The first call on each device looks up the array's device
+ * address and keeps it for the life of the process; make that call before any
+ * stream capture begins, and do not use this entry point across a
+ * cudaDeviceReset, after which the kept address is stale. All calls share the
+ * one array: two calls whose work can overlap on the GPU (different queues
+ * with no event ordering them) race on it, while calls on one queue are safe.
+ * Each call writes every part of the array it reads, so nothing has to be
+ * cleared between calls. The call allocates nothing. */
 int fb_zgram_static(fb_z128* C, int64_t ldc,
                     const fb_z128* A, int64_t lda, const fb_z128* B, int64_t ldb,
                     int64_t rows, int kA, int kB, fb_z128 alpha, fb_z128 beta, fb_queue_t queue);
@@ -218,6 +221,36 @@ int fb_zcholqr2(fb_z128* Y, int64_t ldy, int64_t N, int k,
                 void* workspace, size_t workspace_bytes, fb_queue_t queue);
 int fb_zcholqr2_query(const void* workspace, int* info, int* passes,
                       double* shifts /* 3 entries, or NULL */);
+
+/* cholqr2!(Y) (src/panelblas.jl:130-146) end to end for a matrix held in
+ * page-locked host panels (the resident path of a PanelMatrix whose panels
+ * live on the host tier, src/panels.jl:365-458, narrowed tiers included,
+ * src/panels.jl:94-122): panel p holds panel_cols[p] consecutive columns,
+ * column major with leading dimension host_ld[p] >= N, of element type
+ * host_type (FB_C128, or FB_C64 for a ComplexF32 tier); the panels together
+ * hold the k columns in order. Y (device, N x k ComplexF64, leading dimension
+ * ldy) is the staging copy. The panels go up in row blocks on a library-owned
+ * stream while pass 1's Gram consumes the blocks already landed (narrow
+ * blocks widened on the device first); the last triangular solve runs block
+ * by block, each solved block going back into the panels (narrowed on the
+ * device) on a second stream while the next is solved. All arithmetic is
+ * FP64. shift_unit_roundoff = 0 runs cholqr2!; u in (0, 1) runs the shifted
+ * CholeskyQR3 of fb_zcholqr3_shifted with that unit roundoff. Q replaces Y in
+ * the panels and R (device) is as in fb_zcholqr2; for ComplexF64 panels both
+ * equal fb_zcholqr2's (fb_zcholqr3_shifted's) on the same matrix to the bit.
+ * Synchronizes: it reads the chain's status once after pass 2 (and after
+ * pass 3) and returns when Q is in the panels. A chain that stops on a Gram
+ * that is not positive definite writes nothing back (the panels keep Y) and
+ * returns FB_ENOTSPD with *info set. Workspace:
+ * fb_zcholqr2_staged_workspace_size bytes, 256-byte aligned (the chain's, plus
+ * two narrow staging blocks for FB_C64). fb_zcholqr2_staged_blocks gives the
+ * number of row blocks. */
+int fb_zcholqr2_staged_blocks(int64_t N, int k, int* blocks);
+int fb_zcholqr2_staged_workspace_size(int64_t N, int k, int host_type, size_t* bytes);
+int fb_zcholqr2_staged(void* const* host_panels, int host_type, const int64_t* host_ld, const int* panel_cols,
+                       int npanels, fb_z128* Y, int64_t ldy, int64_t N, int k, fb_z128* R, int64_t ldr,
+                       double shift_unit_roundoff, int* info, int* passes, void* workspace, size_t workspace_bytes,
+                       fb_queue_t queue);
 
 /* The shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Zhang, Yamamoto,
  * SIAM J. Sci. Comput. 2020), the orthonormalization the north-star backend

@@ -12,13 +12,23 @@
  *   complex: sqrt(-ln u1) (cos 2 pi u2, sin 2 pi u2);  real: sqrt(-2 ln u1) cos 2 pi u2
  *
  * Philox4x32-10 follows Salmon et al., SC 2011 (checked here against the
- * published known-answer vectors). ln, cos and sin are series with 1/n and
- * 1/n! coefficients evaluated with explicit fma; build with
+ * published known-answer vectors). ln and cos/sin are table driven:
+ *   ln x, x = 2^e m, m in (sqrt(1/2), sqrt(2)]: bin of m's top 8 fraction bits
+ *     gives (inv, lninv) with lninv = ln(1/inv); r = fma(m, inv, -1);
+ *     ln x = fma(e, ln2_hi, lninv) + fma(e, ln2_lo, log1p(r)), log1p to r^8;
+ *   cos/sin of 2 pi u, u = b 2^-53: bin j = b >> 45 gives (cos, sin) of its
+ *     centre; the rest a = 2 pi (u - centre) by series to a^7 and a^6 and the
+ *     angle sum.
+ * The tables come from the product's generated fb_ghost_tables.h (constants
+ * only; every operation is restated here), so both round alike. Build with
  * -ffp-contract=off so nothing else is contracted.
  * Parity with the reference's values: unpinned (see above). */
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+
+#define FB_GHOST_TABLE_QUALIFIER static const
+#include "../funicular.jl_b200/csrc/fb_ghost_tables.h"
 
 static void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1) {
     const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
@@ -57,46 +67,36 @@ static double ln_pos(double x) {
         m = m * 0.5;
         e += 1;
     }
-    const double f = m - 1.0;
-    const double s = f / (2.0 + f);
-    const double z = s * s;
-    static const double inv_odd[9] = {1.0 / 19.0, 1.0 / 17.0, 1.0 / 15.0, 1.0 / 13.0, 1.0 / 11.0,
-                                      1.0 / 9.0,  1.0 / 7.0,  1.0 / 5.0,  1.0 / 3.0};
-    double p = inv_odd[0];
-    for (int i = 1; i < 9; ++i) p = fma(p, z, inv_odd[i]);
-    const double t = s + s;
-    const double lnm = fma(t * z, p, t);
-    return fma((double)e, 0.6931471805599453, lnm);
+    uint64_t m_bits;
+    memcpy(&m_bits, &m, sizeof m_bits);
+    const int j = (int)((m_bits >> 44) & 0xff);
+    const int idx = m >= 1.0 ? j : FB_GHOST_LN_UPPER_BINS + (j - FB_GHOST_LN_LOWER_FIRST);
+    const double inv = fb_ghost_ln_table[2 * idx], lninv = fb_ghost_ln_table[2 * idx + 1];
+    const double r = fma(m, inv, -1.0);
+    /* log1p(r) = r + r^2 (-1/2 + r (1/3 + r (-1/4 + ... - r/8))) */
+    static const double coef[7] = {-1.0 / 8.0, 1.0 / 7.0, -1.0 / 6.0, 1.0 / 5.0, -1.0 / 4.0, 1.0 / 3.0, -0.5};
+    double p = coef[0];
+    for (int i = 1; i < 7; ++i) p = fma(p, r, coef[i]);
+    const double l1p = fma(r * r, p, r);
+    const double hi = fma((double)e, FB_GHOST_LN2_HI, lninv);
+    const double lo = fma((double)e, FB_GHOST_LN2_LO, l1p);
+    return hi + lo;
 }
 
-static void cos_sin_2pi(double u, double* c, double* s) {
-    const double t = 4.0 * u;
-    const double qf = floor(t + 0.5);
-    const double r = t - qf;
-    const int q = ((int)qf) & 3;
-    const double a = r * 1.5707963267948966;
+static void cos_sin_2pi(uint64_t b, double* c, double* s) {
+    const int j = (int)(b >> 45);
+    const long long f = (long long)(b & ((1ULL << 45) - 1)) - (1LL << 44);
+    const double a = ((double)f * 0x1.0p-53) * FB_GHOST_TWO_PI;
     const double a2 = a * a;
-    /* sin: a + a^3 (-1/3! + a^2 (1/5! - ...)), down from 1/17!. */
-    static const double sin_coef[8] = {1.0 / 355687428096000.0, -1.0 / 1307674368000.0, 1.0 / 6227020800.0,
-                                       -1.0 / 39916800.0,       1.0 / 362880.0,         -1.0 / 5040.0,
-                                       1.0 / 120.0,             -1.0 / 6.0};
-    /* cos: 1 - a^2/2 + a^4 (1/4! - a^2 (1/6! - ...)), down from -1/18!. */
-    static const double cos_coef[8] = {-1.0 / 6402373705728000.0, 1.0 / 20922789888000.0, -1.0 / 87178291200.0,
-                                       1.0 / 479001600.0,         -1.0 / 3628800.0,       1.0 / 40320.0,
-                                       -1.0 / 720.0,              1.0 / 24.0};
-    double sp = sin_coef[0], cp = cos_coef[0];
-    for (int i = 1; i < 8; ++i) {
-        sp = fma(sp, a2, sin_coef[i]);
-        cp = fma(cp, a2, cos_coef[i]);
-    }
-    const double sa = fma(a * a2, sp, a);
-    const double ca = fma(a2 * a2, cp, fma(a2, -0.5, 1.0));
-    switch (q) {
-        case 0: *c = ca; *s = sa; break;
-        case 1: *c = -sa; *s = ca; break;
-        case 2: *c = -ca; *s = -sa; break;
-        default: *c = sa; *s = -ca; break;
-    }
+    double ps = fma(a2, -1.0 / 5040.0, 1.0 / 120.0);
+    ps = fma(ps, a2, -1.0 / 6.0);
+    const double sa = fma(a * a2, ps, a);
+    double pc = fma(a2, -1.0 / 720.0, 1.0 / 24.0);
+    pc = fma(pc, a2, -0.5);
+    const double cm1 = a2 * pc;
+    const double C = fb_ghost_trig_table[2 * j], S = fb_ghost_trig_table[2 * j + 1];
+    *c = C + fma(C, cm1, -(S * sa));
+    *s = S + fma(S, cm1, C * sa);
 }
 
 /* Entry (row, col) of the ghost matrix as (re, im); im = 0 for a real one.
@@ -110,9 +110,8 @@ void ghost_oracle_entry(uint64_t seed, int64_t row, int64_t col, int is_complex,
     const uint64_t a = ((uint64_t)x[0] << 32) | x[1];
     const uint64_t b = ((uint64_t)x[2] << 32) | x[3];
     const double u1 = (double)((a >> 11) + 1) * 0x1.0p-53;
-    const double u2 = (double)(b >> 11) * 0x1.0p-53;
     double c, s;
-    cos_sin_2pi(u2, &c, &s);
+    cos_sin_2pi(b >> 11, &c, &s);
     const double l = ln_pos(u1);
     double re, im;
     if (is_complex) {
@@ -151,4 +150,7 @@ void ghost_oracle_fill(double* dst, int64_t ld, int64_t rows, int64_t cols, int6
 /* The ln and cos/sin above, exposed for accuracy tests against libm. */
 double ghost_oracle_ln(double x) { return ln_pos(x); }
 
-void ghost_oracle_cos_sin_2pi(double u, double out[2]) { cos_sin_2pi(u, &out[0], &out[1]); }
+/* u must be a multiple of 2^-53 in [0, 1), as every u2 of the fill is. */
+void ghost_oracle_cos_sin_2pi(double u, double out[2]) {
+    cos_sin_2pi((uint64_t)(u * 0x1.0p53), &out[0], &out[1]);
+}

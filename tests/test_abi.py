@@ -175,3 +175,23 @@ def test_newer_entry_points_check_arguments_without_a_gpu(fb):
     assert lib.fb_tune_set_batch_lanes(17) == E.FB_EINVAL
     assert lib.fb_tune_set_gram_chunks(100, 4, 9) == E.FB_EINVAL
     assert lib.fb_tune_set_gram_chunks(0, 4, 1) == E.FB_EINVAL
+
+
+def test_static_gram_scratch_holds_every_gram_of_at_most_128_columns(fb):
+    """fb_zgram_static keeps its partial tiles in a 32 MiB array. A partial
+    tile takes tw_a x tw_b entries, so narrow panels over many rows (many row
+    chunks, few entries each) stay small; the documented bound is that every
+    Gram of at most 128 columns a side fits on a 148-SM B200 (the SM count the
+    library assumes without a device)."""
+    if fb._lib.device_count() > 0:
+        pytest.skip("the bound is stated for the 148 SMs the library assumes without a device")
+    need = ctypes.c_size_t(0)
+    worst = 0
+    for rows in (1000, 16_384, 200_003, 1_000_000, 10_000_000, 40_001_688, 1 << 30):
+        for kA in range(1, 129):
+            for kB in sorted({kA, 1, 8, 16, 64, 128}):
+                for herm in ((0, 1) if kA == kB else (0,)):
+                    fb._lib.call("fb_zgram_workspace_size", ctypes.c_int64(rows), kA, kB, herm,
+                                 ctypes.byref(need))
+                    worst = max(worst, need.value)
+    assert worst <= 32 << 20

@@ -126,7 +126,8 @@ def test_rdiv_upper_complex_diagonal(fb, backend, oracle):
     np.testing.assert_allclose(Yd.to_host(), expect, rtol=1e-13)
 
 
-@pytest.mark.parametrize("rows,s,r", [(12, 5, 4), (1000, 64, 64), (77, 3, 100), (500, 80, 7), (9, 1, 1)])
+@pytest.mark.parametrize("rows,s,r", [(12, 5, 4), (1000, 64, 64), (77, 3, 100), (500, 80, 7), (9, 1, 1),
+                                      (100_003, 64, 64), (20_001, 200, 130), (5000, 17, 64), (4097, 64, 9)])
 def test_rightmul_gemm(fb, backend, oracle, rows, s, r):
     rng = np.random.default_rng(rows + s + r)
     A, C = randmatrix(rng, rows, s), randmatrix(rng, s, r)

@@ -405,9 +405,34 @@ def test_project_against_dense(fb, backend, plan, rng, w, nb):
     Q = fb.PanelMatrix.from_array(A, plan=plan, w=w)
     ref = A.conj().T @ G @ A
     tol = blastol(N, k)
-    assert close(fb.project(Q, dense, nbuffers=nb), ref, tol)
-    assert close(fb.project(Q, fb.ColumnOperator(dense), nbuffers=nb), ref, tol)
+    for schedule in (None,) + fb.panelblas.PROJECT_SCHEDULES:
+        assert close(fb.project(Q, dense, nbuffers=nb, schedule=schedule), ref, tol), schedule
+        assert close(fb.project(Q, fb.ColumnOperator(dense), nbuffers=nb, schedule=schedule), ref, tol), schedule
     assert np.array_equal(Q.to_array(), A)
+
+
+def test_project_schedule_follows_the_budgets(fb, backend, make_plan, rng):
+    """Resident when Q and G Q fit the device budget, two sweeps when only a
+    second matrix fits on the host, nested (the reference's) when neither;
+    all three give the same S."""
+    N, k, w = 20_000, 48, 4
+    L = fb.Laplacian7((50, 40, 10), 0.5 + 0.1j)
+    A = randmatrix(rng, N, k)
+    nbytes = N * k * 16
+    # Room for the sweeps' staging buffers (the pool keeps those of both of
+    # the two-sweep schedule's sweeps, 10.3 MB), not for Q and G Q together.
+    small = 12 * MiB
+    cases = {"resident": make_plan(device_budget=4 * nbytes, host_budget=4 * nbytes, panel_width=w),
+             "two-sweep": make_plan(device_budget=small, host_budget=4 * nbytes, panel_width=w),
+             "nested": make_plan(device_budget=small, host_budget=nbytes + MiB, panel_width=w)}
+    results = {}
+    for want, p in cases.items():
+        Q = fb.PanelMatrix.from_array(A, plan=p)
+        assert fb.panelblas.project_schedule(Q) == want
+        results[want] = fb.project(Q, L)
+    tol = blastol(N, k)
+    assert close(results["two-sweep"], results["nested"], tol)
+    assert close(results["resident"], results["nested"], tol)
 
 
 def test_project_matches_panelmul_followed_by_gram(fb, backend, plan, rng):

@@ -4,9 +4,10 @@ It exists for callers that have no device memory to hand over as a workspace
 (a host whose allocator has promised every device byte to a budgeted pool, or
 one that must not pay for cudaMalloc inside a pipelined sweep), so it keeps its
 scratch in a fixed array inside the library. This test calls it through the C
-ABI and checks it against fb_zgram, the workspace-taking entry point, twice in
-a row, so that the second call also shows the shared scratch carries nothing
-over from the first. The file is named to be collected last.
+ABI and checks it against fb_zgram, the workspace-taking entry point, bit for
+bit, twice in a row, so that the second call also shows the shared scratch
+carries nothing over from the first, and checks that repeated calls leave the
+device's free memory unchanged. The file is named to be collected last.
 """
 import ctypes
 
@@ -41,10 +42,14 @@ def gram_with_workspace(fb, backend, C, A, B, alpha, beta):
     fb._lib.call("fb_sync_all")
 
 
-@pytest.mark.parametrize("rows,kA,kB,same", [(200_003, 64, 64, True), (4099, 23, 9, False), (50_000, 128, 128, True)])
-def test_static_scratch_matches_the_workspace_entry_point(fb, backend, oracle, rows, kA, kB, same):
+# Shapes: a folded 64-column Gram, a cross Gram of ragged widths, a 128-column
+# Gram (three 64 x 64 tiles), and narrow panels over many rows, whose many
+# row chunks each keep a partial tile of only 8 x 8 or 16 x 16 entries.
+@pytest.mark.parametrize("rows,kA,kB,same", [(200_003, 64, 64, True), (4099, 23, 9, False), (50_000, 128, 128, True),
+                                             (200_003, 8, 8, True), (1_000_000, 16, 16, True),
+                                             (1_000_000, 8, 16, False)])
+def test_static_scratch_matches_the_workspace_entry_point(fb, backend, rows, kA, kB, same):
     rng = np.random.default_rng(rows + kA)
-    tol = oracle.blastol(np.complex128, rows, kA)
     for call in range(2):
         A = randmatrix(rng, rows, kA)
         B = A if same else randmatrix(rng, rows, kB)
@@ -55,11 +60,30 @@ def test_static_scratch_matches_the_workspace_entry_point(fb, backend, oracle, r
         gram_with_workspace(fb, backend, expect, Ad, Bd, 1.0, 0.0)
         gram_static(fb, got, Ad, Bd, 1.0, 0.0)
         fb._lib.call("fb_sync_all")
-        np.testing.assert_allclose(got.to_host(), expect.to_host(), rtol=tol, atol=tol)
-        # beta = 1 accumulates onto what the first product left.
+        # Same partial tiles, same reduction order: the same bits.
+        np.testing.assert_array_equal(got.to_host(), expect.to_host())
+        # beta = 1 accumulates onto what the first product left, as fb_zgram does.
+        gram_with_workspace(fb, backend, expect, Ad, Bd, 0.5, 1.0)
         gram_static(fb, got, Ad, Bd, 0.5, 1.0)
         fb._lib.call("fb_sync_all")
-        np.testing.assert_allclose(got.to_host(), 1.5 * expect.to_host(), rtol=tol, atol=tol)
+        np.testing.assert_array_equal(got.to_host(), expect.to_host())
+
+
+def test_static_scratch_call_allocates_no_device_memory(fb, backend):
+    import torch
+
+    rows, k = 300_000, 64
+    rng = np.random.default_rng(7)
+    Ad = backend.todevice(randmatrix(rng, rows, k))
+    C = backend.alloc_device(np.complex128, (k, k))
+    gram_static(fb, C, Ad, Ad, 1.0, 0.0)  # warm: the kernels are loaded by now
+    fb._lib.call("fb_sync_all")
+    free_before, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        gram_static(fb, C, Ad, Ad, 1.0, 0.0)
+    fb._lib.call("fb_sync_all")
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
 
 
 def test_static_scratch_refuses_shapes_that_do_not_fit(fb, backend):

@@ -301,11 +301,13 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
     };
     // The Y blocks of the next two steps are always in flight: a step is one
     // column block of one unit, and the prefetch runs on into the warp's next
-    // unit.
+    // units. Block b of a unit is read from slot b & 1; with an odd block
+    // count the prefetch leaves the next unit's blocks 0 and 1 in slots 1 and
+    // 0, so the slots are swapped at the end of each unit.
     int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
     z64 yq[2][2];
     load_y(u, 0, yq[0]);
-    if (NBLK > 1) load_y(u, 1, yq[1]); else load_y(u + warps_total, 0, yq[1]);
+    load_y(u + (1 / NBLK) * warps_total, 1 % NBLK, yq[1]);
     for (; u < units; u += warps_total) {
         const int64_t row = u * 8 + rr;
         const bool live = row < rows;
@@ -324,8 +326,7 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
                 for (int h = 1; h < NCH; ++h) acc[h][t][0] = acc[h][t][1] = 0.0;
             }
             // Refill the slot just consumed with the block two steps ahead.
-            if (b + 2 < NBLK) load_y(u, b + 2, yq[slot]);
-            else load_y(u + warps_total, b + 2 - NBLK, yq[slot]);
+            load_y(u + ((b + 2) / NBLK) * warps_total, (b + 2) % NBLK, yq[slot]);
             // Y_b - sum_{c<b} X_c R_cb, k-steps spread over NCH accumulators.
 #pragma unroll
             for (int c = 0; c < b; ++c) {
@@ -374,6 +375,14 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
                 for (int s = 0; s < 4; ++s)
                     xa[b][s] = reinterpret_cast<const double*>(&buf[tbuf_index(rr, 2 * s + acol)])[apart];
                 __syncwarp();
+            }
+        }
+        if (NBLK & 1) {
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const z64 tmp = yq[0][t];
+                yq[0][t] = yq[1][t];
+                yq[1][t] = tmp;
             }
         }
     }

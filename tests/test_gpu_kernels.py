@@ -323,6 +323,38 @@ def test_rdiv_upper_both_tensor_core_paths(fb, backend, oracle, k, scale):
     assert np.linalg.norm(X @ R - Y) <= 1e-14 * np.linalg.norm(Y) * max(1.0, np.sqrt(cond))
 
 
+@pytest.mark.parametrize("k", [8, 24, 37, 40, 56, 64])
+def test_rdiv_upper_blocked_solve_over_many_sweeps(fb, backend, oracle, k):
+    # Enough rows that every warp solves several 8-row units in turn (the
+    # grid covers about 3e4 rows a sweep), with odd and even counts of 8-column
+    # blocks: the Y prefetch runs from one unit into the next.
+    rng = np.random.default_rng(k + 1000)
+    rows = 300_001
+    Y = randmatrix(rng, rows, k)
+    R = np.asfortranarray(np.eye(k) + 0.5 * np.triu(randmatrix(rng, k, k)))
+    Yd, Rd = backend.todevice(Y), backend.todevice(R)
+    fb.kernels.rdiv_upper(backend, Yd, Rd)
+    expect = Y.copy(order="F")
+    oracle.rdiv_upper(expect, R)
+    X = Yd.to_host()
+    cond = np.linalg.norm(R, 1) * np.linalg.norm(np.linalg.inv(R), 1)
+    np.testing.assert_allclose(X, expect, rtol=0, atol=1e-14 * cond * np.abs(expect).max())
+    assert np.linalg.norm(X @ R - Y) <= 1e-14 * np.linalg.norm(Y) * max(1.0, np.sqrt(cond))
+
+
+@pytest.mark.parametrize("k", [24, 40])
+def test_cholqr2_resident_odd_block_counts(fb, backend, oracle, k):
+    rng = np.random.default_rng(k)
+    N = 200_003
+    A = conditioned(rng, N, k, 1e3)
+    Y = backend.todevice(A)
+    R = nanbuffer(backend, (k, k))
+    fb.kernels.cholqr2_resident(backend, Y, R)
+    Q, Rh = Y.to_host(), R.to_host()
+    assert oracle.orthogonality_error(Q) <= 1e-12
+    assert oracle.reconstruction_error(A, Q, Rh) <= 1e-13
+
+
 @pytest.mark.parametrize("kappa", [1e4, 1e7])
 def test_cholqr2_resident_k128_conditioned(fb, backend, oracle, kappa):
     # Past 64 columns the triangular solves go by 64-column blocks, each

@@ -686,6 +686,8 @@ def run_project(args, fb, backend, torch, device, world, max_over_ranks, barrier
     roof_ms = max(nbytes / (hbm_peak * 1e9), flops / (fp64_peak * 1e12)) * 1e3
     # End to end through the public API.
     Qh = np.asfortranarray(Q.to_host())
+    del Q, Z
+    release_device_memory(torch)
     plan = fb.ResidencyPlan(device_budget=3 * N * k * 16 + fb.GiB, host_budget=N * k * 16 + 64 * 2 ** 20,
                             backend=backend, panel_width=16)
     Qpm = fb.PanelMatrix.from_array(Qh, plan=plan)
@@ -699,7 +701,7 @@ def run_project(args, fb, backend, torch, device, world, max_over_ranks, barrier
             times.append(time.perf_counter() - t0)
     ms_e2e = max_over_ranks(1e3 * sum(times) / len(times))
     fb.free(Qpm)
-    del Qh, Qpm, plan, Q, Z
+    del Qh, Qpm, plan
     return {"workload": f"project(Q, G), N={N} (215^3 Laplacian, shift 0.5+0.1i), k={k}, device-resident",
             "cross_gram": {"ms": ms_gram, "tflops": flops / (ms_gram * 1e-3) / 1e12,
                            "gbs": nbytes / (ms_gram * 1e-3) / 1e9, "ms_roofline": roof_ms, "frac": roof_ms / ms_gram,
@@ -813,6 +815,15 @@ def run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier
         "band_apply": {"ms": ms_band, "tflops": flops_band / (ms_band * 1e-3) / 1e12,
                        "per_launch": "8 N k (2 kd + 1) flops"},
     }
+
+
+def release_device_memory(torch) -> None:
+    """Frees what dropped Python references held: the backend's buffers (their
+    finalizers run on collection) and the blocks torch's allocator caches."""
+    import gc
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
 
 
 def reduce_max_over_ranks(x: float, world: int, device) -> float:
@@ -1104,22 +1115,22 @@ def run_ours(args):
         "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_source, "fp64_peak_tflops": fp64_peak,
     }
 
-    c1, c1_outputs = (run_c1(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
-                      if args.c1_N > 0 else (None, None))
+    def section(run, *extra):
+        # Each section allocates both through the backend and through torch;
+        # what a finished section held goes back to the device before the
+        # next one (torch's caching allocator would otherwise keep it).
+        out = run(args, fb, backend, torch, device, world, max_over_ranks, barrier, *extra)
+        release_device_memory(torch)
+        return out
 
-    batched = (run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
-               if args.batch > 0 else None)
-
-    wide = (run_wide(args, fb, backend, torch, device, world, max_over_ranks, barrier, fp64_peak)
-            if args.wide_N > 0 else None)
+    c1, c1_outputs = section(run_c1, hbm_peak, fp64_peak) if args.c1_N > 0 else (None, None)
+    batched = section(run_batched, hbm_peak, fp64_peak) if args.batch > 0 else None
+    wide = section(run_wide, fp64_peak) if args.wide_N > 0 else None
     if wide is not None and args.e2e_steps > 0:
-        wide["storage"] = run_wide_storage(args, fb, backend, torch, device, world, max_over_ranks, barrier)
-    range_finder = (run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, barrier)
-                    if args.rf_k > 0 else None)
-    project = (run_project(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak)
-               if args.project_k > 0 else None)
-    adjoint = (run_adjoint(args, fb, backend, torch, device, world, max_over_ranks, barrier)
-               if args.adjoint_N > 0 else None)
+        wide["storage"] = section(run_wide_storage)
+    range_finder = section(run_range_finder) if args.rf_k > 0 else None
+    project = section(run_project, hbm_peak, fp64_peak) if args.project_k > 0 else None
+    adjoint = section(run_adjoint) if args.adjoint_N > 0 else None
     if adjoint is not None:
         fp = adjoint["cholqr2_pullback"]["tflops"]
         adjoint["cholqr2_pullback"]["fp64_frac"] = fp / fp64_peak

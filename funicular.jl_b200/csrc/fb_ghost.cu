@@ -65,11 +65,14 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], const RoundKeys& rk
 constexpr int LN_DOUBLES = 2 * FB_GHOST_LN_ENTRIES;
 constexpr int TRIG_DOUBLES = 2 * 256;
 
-// ln x for a positive normal x: x = 2^e m with m in (sqrt(1/2), sqrt(2)].
-__device__ __forceinline__ double ln_pos(double x, const double* __restrict__ lnt) {
-    const long long bits = __double_as_longlong(x);
-    int e = (int)((bits >> 52) & 0x7ff) - 1023;
-    double m = __longlong_as_double((bits & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+// ln u for u = n 2^-53, 1 <= n <= 2^53, read straight from the integer (the
+// exponent and fraction bits u has as a double, without converting):
+// u = 2^e m with m in (sqrt(1/2), sqrt(2)].
+__device__ __forceinline__ double ln_u53(uint64_t n, const double* __restrict__ lnt) {
+    const int lz = __clzll((long long)n);
+    int e = 10 - lz;                                          // 63 - lz - 53
+    const uint64_t frac = ((n << lz) >> 11) & 0x000fffffffffffffull;
+    double m = __longlong_as_double((long long)(frac | 0x3ff0000000000000ull));
     if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
     const int j = (int)((__double_as_longlong(m) >> 44) & 0xff);
     const int idx = m >= 1.0 ? j : FB_GHOST_LN_UPPER_BINS + (j - FB_GHOST_LN_LOWER_FIRST);
@@ -107,12 +110,13 @@ __device__ __forceinline__ void cos_sin_2pi(uint64_t b, const double* __restrict
     s = S + fma(S, cm1, C * sa);
 }
 
-__device__ __forceinline__ void uniforms(const RoundKeys& rk, int64_t row, int64_t col, double& u1, uint64_t& b2) {
+// The two 53-bit integers of an entry: u1 = n1 2^-53 in (0, 1], u2 = b2 2^-53.
+__device__ __forceinline__ void uniforms(const RoundKeys& rk, int64_t row, int64_t col, uint64_t& n1, uint64_t& b2) {
     uint32_t c[4] = {(uint32_t)row, (uint32_t)((uint64_t)row >> 32), (uint32_t)col, (uint32_t)((uint64_t)col >> 32)};
     philox4x32_10(c, rk);
     const uint64_t a = ((uint64_t)c[0] << 32) | c[1];
     const uint64_t b = ((uint64_t)c[2] << 32) | c[3];
-    u1 = (double)((a >> 11) + 1) * 0x1.0p-53;
+    n1 = (a >> 11) + 1;
     b2 = b >> 11;
 }
 
@@ -140,11 +144,11 @@ __global__ void __launch_bounds__(256) ghost_fill_kernel(D* __restrict__ dst, in
     for (int64_t j = blockIdx.y; j < cols; j += gridDim.y) {
         D* column = dst + j * ld;
         for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) {
-            double u1, c, s;
-            uint64_t b2;
-            uniforms(rk, row0 + i, col0 + j, u1, b2);
+            double c, s;
+            uint64_t n1, b2;
+            uniforms(rk, row0 + i, col0 + j, n1, b2);
             cos_sin_2pi(b2, trig, c, s);
-            const double l = ln_pos(u1, lnt);
+            const double l = ln_u53(n1, lnt);
             double re, im;
             if (COMPLEX) {
                 const double rad = sqrt(-l);

@@ -3,17 +3,15 @@
 // entry into 8-bit slices whose products are exact in 32-bit integer
 // accumulators, recovered to FP64 with power-of-two weights.
 //
-// Real form. W is the 2N x k real matrix holding Re Y and Im Y in
-// alternating rows (exactly the interleaved ComplexF64 layout of a column);
-// V is W with every Re row set to zero and every Im row moved up onto the Re
-// row above it (V[2r] = Im y_r, V[2r+1] = 0). Then
-//   W^T W = Re G,   V^T W = P with P[a][b] = sum_r Im y_ra Re y_rb,
-// and Im G[a][b] = P[b][a] - P[a][b]. The MMA operand A holds the slices of
-// W (rows 0-63) and V (rows 64-127) in tensor memory, so one 128 x 64 product
-// per slice pair gives both; operand B holds the W slices stacked along N in
-// shared memory, so one MMA of A slice t against B slices 1..7-t lands in the
-// accumulators of the groups g = t + u it feeds. V's slices are W's slices
-// with bytes moved (one byte permute a word): every FP64 value is sliced once.
+// Real form. With W the 2N x k real matrix holding Re Y and Im Y in
+// alternating rows (exactly the interleaved ComplexF64 layout of a column) and
+// JW the same with each (re, im) pair turned into (im, -re):
+//   [W JW]^T W = [Re G ; -Im G]      (a 128 x 64 product for k <= 64).
+// The MMA operand A holds the slices of W and JW, 128 rows, in tensor memory;
+// operand B holds the W slices stacked along N in shared memory, so one MMA
+// of A slice t against B slices 1..7-t lands in the accumulators of the groups
+// g = t + u it feeds. Keeping A in tensor memory halves the shared-memory
+// traffic of the products, which bounds this kernel.
 //
 // Slices. Column j carries a power-of-two scale 2^E_j with |entries| <
 // 2^(E_j - 1); an entry x becomes the integer x_int = rint(x 2^(51 - E_j)),
@@ -26,17 +24,8 @@
 // slices are read straight out of the double's bit pattern, and its exponent
 // field tells whether x was in range. A product of two entries is
 // 2^(E_a + E_b - 102) sum_{t,u} d_t e_u 2^(104 - 8 (t + u)); the 28 terms
-// with t + u <= 8 are kept, the rest lie below 2^-50 of the leading term.
-// Group g = t + u owns 64 accumulator columns of tensor memory (448 in all),
-// the A slices the next 56.
-//
-// Pipeline. A has one copy in tensor memory, so it is handed over in two
-// parts: slices 1-3 (64 % of a stage's MMA work) and slices 4-7. The MMAs of
-// each part are committed to their own barrier, and the slicers write a part
-// of the next stage as soon as that barrier says the previous stage's MMAs
-// have read it, while the tensor core works on the other part. (One part per
-// slice was measured slower: seven store round trips per stage in every
-// slicer warp.) B has two buffers. Barriers are arrived on once per warp.
+// with t + u <= 8 are kept, the rest lie below 2^-50 of the leading term. Group g = t + u owns 64 accumulator columns of tensor memory (448 in
+// all), the A slices the next 56.
 //
 // Scales adapt as the rows stream: a stage with an entry its column's scale
 // cannot hold, or one that would let an int32 accumulator overflow (every
@@ -46,10 +35,8 @@
 // deterministic.
 //
 // Rows of A (tensor memory lanes): lane 32q + l holds W column 16q + l for
-// l < 16 and V column 16q + l - 16 for l >= 16. Of a warp's thread pair
-// (l, l + 16) for column j, the first slices complex rows 0-1 and the second
-// rows 2-3 of its four rows of the stage; they swap their slice words with
-// one shuffle each, and the first writes W, the second V.
+// l < 16 and JW column 16q + l - 16 for l >= 16, so one warp writes both rows
+// of a column and its two halves read the same FP64 values (a broadcast).
 //
 // Roles (one CTA per SM, 576 threads): warps 0-15 slice (warp w writes lane
 // quarter w % 4, K bytes 8 (w / 4)..+7 of every A slice) and drain (lane
@@ -78,14 +65,10 @@ constexpr int THREADS = SLICERS + 64;
 // in the mantissa of a double whose high word starts with 0x433.
 constexpr long long MAGIC_BITS = 0x4338080808080808ll;
 
-constexpr int SLICER_WARPS = SLICERS / 32;
-constexpr int PARTS = 2;                        // A is handed over in two parts of slices
-__host__ __device__ constexpr int part_first(int h) { return h == 0 ? 0 : h == 1 ? 3 : SLICES; }
-
 constexpr size_t OFF_F = 0;
 constexpr size_t OFF_B = OFF_F + (size_t)FSTAGES * FBYTES;
-constexpr size_t OFF_MAX = OFF_B + (size_t)SBUFS * BTILE;   // uint32 [8][64] column maxima
-constexpr size_t OFF_BAR = OFF_MAX + 8 * 64 * 4;            // mbarriers
+constexpr size_t OFF_MAX = OFF_B + (size_t)SBUFS * BTILE;   // uint32 [4][64] column maxima
+constexpr size_t OFF_BAR = OFF_MAX + 4 * 64 * 4;            // mbarriers
 constexpr size_t OFF_MISC = OFF_BAR + 32 * 8;
 constexpr size_t MISC_BYTES = 512;                          // flags, TMEM slot, column exponents
 constexpr size_t SMEM_BYTES = OFF_MISC + MISC_BYTES + 1024;  // + alignment slack
@@ -146,11 +129,10 @@ __device__ __forceinline__ void slice_words(const uint64_t (&y)[4], uint32_t (&w
 // at tcol (this thread's lane, column 16c of group 0). False if the MMAs
 // never finished. Kept out of line: it runs a few times per CTA and would
 // otherwise hold registers across the slicing loop.
-__device__ __noinline__ bool drain_epoch(uint64_t* last_slice_done, int last_stage, uint32_t tcol, const int* Es,
-                                         int prow, int c, double* P, bool initialized) {
-    // Every MMA up to last_stage has finished once the commit of its last
-    // slice arrived (one phase of that barrier per stage).
-    if (!mbar_wait(last_slice_done, last_stage & 1)) return false;
+__device__ __noinline__ bool drain_epoch(uint64_t* sl_empty, int last_stage, uint32_t tcol, const int* Es, int prow,
+                                         int c, double* P, bool initialized) {
+    // Every MMA up to last_stage has finished once its commit arrived.
+    if (!mbar_wait(&sl_empty[last_stage % SBUFS], (last_stage / SBUFS) & 1)) return false;
     umma::fence_after_sync();
     const int Em = Es[prow & 63];
     double acc[16];
@@ -185,10 +167,9 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t* fp_full = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
-    uint64_t* fp_empty = fp_full + FSTAGES;     // one arrival per slicer warp
-    uint64_t* a_full = fp_empty + FSTAGES;      // [PARTS]: part h of A (and, for h = 0, B) written
-    uint64_t* a_empty = a_full + PARTS;         // [PARTS]: the MMAs of part h have finished
-    uint64_t* b_empty = a_empty + PARTS;        // [SBUFS]: the MMAs reading B buffer b have finished
+    uint64_t* fp_empty = fp_full + FSTAGES;
+    uint64_t* sl_full = fp_empty + FSTAGES;
+    uint64_t* sl_empty = sl_full + SBUFS;
     int* misc = reinterpret_cast<int*>(smem + OFF_MISC);
     volatile int* fresh_flag = misc;           // [SBUFS]
     volatile int* abort_flag = misc + 2;
@@ -205,13 +186,12 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     if (threadIdx.x == 0) {
         for (int b = 0; b < FSTAGES; ++b) {
             mbar_init(&fp_full[b], 1);
-            mbar_init(&fp_empty[b], SLICER_WARPS);
+            mbar_init(&fp_empty[b], SLICERS);
         }
-        for (int h = 0; h < PARTS; ++h) {
-            mbar_init(&a_full[h], SLICER_WARPS);
-            mbar_init(&a_empty[h], 1);
+        for (int b = 0; b < SBUFS; ++b) {
+            mbar_init(&sl_full[b], SLICERS);
+            mbar_init(&sl_empty[b], 1);
         }
-        for (int b = 0; b < SBUFS; ++b) mbar_init(&b_empty[b], 1);
         *abort_flag = 0;
         for (int c = 0; c < 64; ++c) Es[c] = E_UNSET;
         mbar_fence_init();
@@ -222,7 +202,7 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     umma::fence_after_sync();
     const uint32_t taddr = *tmem_slot;
 
-    if (warp == SLICER_WARPS + 1) {
+    if (warp == SLICERS / 32 + 1) {
         // ---- producer: FP64 tiles, two 8-row boxes per stage ----
         if (lane == 0) {
             tma_prefetch_map(&tm);
@@ -247,51 +227,44 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             for (int s = issued > FSTAGES ? issued - FSTAGES : 0; *abort_flag && s < issued; ++s)
                 mbar_wait(&fp_full[s % FSTAGES], (s / FSTAGES) & 1);
         }
-    } else if (warp == SLICER_WARPS) {
+    } else if (warp == SLICERS / 32) {
         // ---- MMA issuer ----
         if (lane == 0) {
-            // The barrier and phase of the last commit, which an abort waits
-            // on before tensor memory is released.
-            uint64_t* last_bar = nullptr;
-            uint32_t last_parity = 0;
-            for (int s = 0; s < nstages && last_bar != reinterpret_cast<uint64_t*>(1); ++s) {
-                const int sb = s % SBUFS;
-                const uint32_t bbase = smem_u32(smem + OFF_B + (size_t)sb * BTILE);
-                bool fresh = false;
-#pragma unroll 1
-                for (int h = 0; h < PARTS; ++h) {
-                    if (!mbar_wait(&a_full[h], s & 1) || *abort_flag) {
-                        atomicExch(&flags->timeout, 1);
-                        *abort_flag = 1;
-                        if (last_bar) mbar_wait(last_bar, last_parity);
-                        last_bar = reinterpret_cast<uint64_t*>(1);
-                        break;
-                    }
-                    umma::fence_after_sync();
-                    if (h == 0) fresh = fresh_flag[sb] != 0;
-                    for (int t = part_first(h); t < part_first(h + 1); ++t) {
-                        const int ntot = 64 * (SLICES - t);
-                        for (int off = 0; off < ntot; off += 256) {
-                            const int n = ntot - off < 256 ? ntot - off : 256;
-                            umma::mma_s8_tmem_a(taddr + 64 * t + off, taddr + A_COL + 8 * t,
-                                                desc_sw32(bbase + off * 32), umma::idesc_s8s8_s32(128, n),
-                                                !(fresh && t == 0));
-                        }
-                    }
-                    umma::commit(&a_empty[h]);
-                    last_bar = &a_empty[h];
-                    last_parity = s & 1;
+            int issued = 0;
+            for (int s = 0; s < nstages; ++s) {
+                const int b = s % SBUFS;
+                if (!mbar_wait(&sl_full[b], (s / SBUFS) & 1) || *abort_flag) {
+                    atomicExch(&flags->timeout, 1);
+                    *abort_flag = 1;
+                    break;
                 }
-                if (last_bar != reinterpret_cast<uint64_t*>(1)) umma::commit(&b_empty[sb]);
+                umma::fence_after_sync();
+                const bool fresh = fresh_flag[b] != 0;
+                const uint32_t bbase = smem_u32(smem + OFF_B + (size_t)b * BTILE);
+#pragma unroll
+                for (int t = 0; t < SLICES; ++t) {
+                    const int ntot = 64 * (SLICES - t);
+#pragma unroll
+                    for (int off = 0; off < ntot; off += 256) {
+                        const int n = ntot - off < 256 ? ntot - off : 256;
+                        umma::mma_s8_tmem_a(taddr + 64 * t + off, taddr + A_COL + 8 * t, desc_sw32(bbase + off * 32),
+                                            umma::idesc_s8s8_s32(128, n), !(fresh && t == 0));
+                    }
+                }
+                umma::commit(&sl_empty[b]);
+                issued = s + 1;
             }
+            // After an abort, wait for the MMAs in flight before tensor memory
+            // is released.
+            if (*abort_flag && issued > 0) mbar_wait(&sl_empty[(issued - 1) % SBUFS], ((issued - 1) / SBUFS) & 1);
         }
     } else {
         // ---- slicers and drains: warps 0..15 ----
         const int tid = threadIdx.x;
         const int q = warp & 3, kq = warp >> 2;
-        const bool vrow = lane >= 16;                        // writes V (rows 2-3 of the four)
+        const bool jw = lane >= 16;
         const int j = 16 * q + (lane & 15);                  // this thread's column
-        const int prow = (vrow ? 64 : 0) + j;                // its row of the 128 x 64 partial
+        const int prow = (jw ? 64 : 0) + j;                  // its row of the 128 x 64 partial
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
         int E = E_UNSET;            // scale exponent of column j
         int epoch_start = 0;
@@ -316,26 +289,23 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
             *abort_flag = 1;
         };
         auto drain = [&](int last_stage) -> bool {
-            const bool ok = drain_epoch(&a_empty[PARTS - 1], last_stage, taddr + lane_base + 16 * kq, Es, prow, kq,
-                                        P, initialized);
+            const bool ok = drain_epoch(sl_empty, last_stage, taddr + lane_base + 16 * kq, Es, prow, kq, P, initialized);
             initialized = true;
             return ok;
         };
-        // Complex rows 4 kq + (0, 1) (first of the pair) or 4 kq + (2, 3)
-        // (second) of column j in stage st: rows 4 (kq & 1) + .. of box kq / 2.
-        auto load = [&](int st, double (&vv)[4]) -> bool {
+        // Complex rows 4 (kq & 1) .. + 3 of column j in box kq / 2 of stage st.
+        auto load = [&](int st, double (&vv)[8]) -> bool {
             const int fb = st % FSTAGES;
             if (!mbar_wait(&fp_full[fb], (st / FSTAGES) & 1)) return false;
             const unsigned char* box = smem + OFF_F + (size_t)fb * FBYTES + (size_t)(kq >> 1) * (FBYTES / 2) + j * 128;
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const int rr = 4 * (kq & 1) + (vrow ? 2 : 0) + r;
+            for (int r = 0; r < 4; ++r) {
+                const int rr = 4 * (kq & 1) + r;
                 const double2 z = *reinterpret_cast<const double2*>(box + ((rr ^ (j & 7)) << 4));
                 vv[2 * r] = z.x;
                 vv[2 * r + 1] = z.y;
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&fp_empty[fb]);
+            mbar_arrive(&fp_empty[fb]);
             return true;
         };
 
@@ -348,23 +318,29 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
         int s = 0;
         for (; s < nstages; ++s) {
             const int sb = s % SBUFS;
-            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            double v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = 0.0;
             const bool landed = load(s, v);
-            // Scale and split: re0 im0 re1 im1, four K values to a word. A
-            // result whose high word does not start 0x433 was out of range.
+            // Scale and split: W rows take re0 im0 re1 im1 .., JW rows
+            // im0 -re0 im1 -re1 .., four K values to a word. A result whose
+            // high word does not start 0x433 was out of range.
             double sc = (E == E_UNSET || bad) ? 0.0 : pow2(51 - E);
-            uint64_t t[4];
+            uint64_t t[8];
             uint32_t range = 0;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                t[c] = (uint64_t)__double_as_longlong(fma(v[c], sc, magic));
-                range |= (uint32_t)(t[c] >> 32) ^ 0x43300000u;
+                const double first = jw ? v[2 * c + 1] : v[2 * c];
+                const double second = jw ? v[2 * c] : v[2 * c + 1];
+                t[2 * c] = (uint64_t)__double_as_longlong(fma(first, sc, magic));
+                t[2 * c + 1] = (uint64_t)__double_as_longlong(fma(second, jw ? -sc : sc, magic));
+                range |= ((uint32_t)(t[2 * c] >> 32) ^ 0x43300000u) | ((uint32_t)(t[2 * c + 1] >> 32) ^ 0x43300000u);
             }
             bool out_of_range = (range & 0xFFF00000u) != 0;
             if (E == E_UNSET) {
                 uint32_t nz = 0;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) nz |= (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FF00000u;
+                for (int i = 0; i < 8; ++i) nz |= (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FF00000u;
                 out_of_range = nz != 0;
             }
             const bool epoch_full = s - epoch_start >= EPOCH_STAGES;
@@ -376,12 +352,10 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
                 // by exponent, and Inf and NaN above every finite value.
                 uint32_t mx = 0;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) mx = max(mx, (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FFFFFFFu);
-                colmax[(2 * kq + (vrow ? 1 : 0)) * 64 + j] = mx;
+                for (int i = 0; i < 8; ++i) mx = max(mx, (uint32_t)(__double_as_longlong(v[i]) >> 32) & 0x7FFFFFFFu);
+                if (!jw) colmax[kq * 64 + j] = mx;
                 asm volatile("bar.sync 1, %0;" ::"n"(SLICERS) : "memory");
-                uint32_t cm = 0;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) cm = max(cm, colmax[i * 64 + j]);
+                const uint32_t cm = max(max(colmax[j], colmax[64 + j]), max(colmax[128 + j], colmax[192 + j]));
                 if (cm >= 0x7FF00000u) bad = true;
                 // A column outgrows its scale when its maximum is no longer
                 // below 2^(E - 1); the new scale leaves HEADROOM bits above it.
@@ -396,59 +370,44 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
                     }
                     if (any(!drained)) { fail(); break; }
                     if (over) E = E == E_UNSET ? need : max(E, need);
-                    if (kq == 0 && !vrow) Es[j] = E;
+                    if (kq == 0 && !jw) Es[j] = E;
                     epoch_start = s;
                     fresh = true;
                     if (any_over) {
                         sc = (E == E_UNSET || bad) ? 0.0 : pow2(51 - E);
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) t[c] = (uint64_t)__double_as_longlong(fma(v[c], sc, magic));
+                        for (int c = 0; c < 4; ++c) {
+                            const double first = jw ? v[2 * c + 1] : v[2 * c];
+                            const double second = jw ? v[2 * c] : v[2 * c + 1];
+                            t[2 * c] = (uint64_t)__double_as_longlong(fma(first, sc, magic));
+                            t[2 * c + 1] = (uint64_t)__double_as_longlong(fma(second, jw ? -sc : sc, magic));
+                        }
                     }
                 }
             }
-            // This thread's slice words (its two complex rows), and its
-            // partner's: the W words of rows 0-1 and 2-3 of the four.
-            uint32_t w[SLICES], o[SLICES];
+            uint32_t w0[SLICES], w1[SLICES];
             {
-                const uint64_t y[4] = {t[0] << 4, t[1] << 4, t[2] << 4, t[3] << 4};
-                slice_words(y, w);
+                const uint64_t y0[4] = {t[0] << 4, t[1] << 4, t[2] << 4, t[3] << 4};
+                const uint64_t y1[4] = {t[4] << 4, t[5] << 4, t[6] << 4, t[7] << 4};
+                slice_words(y0, w0);
+                slice_words(y1, w1);
             }
-#pragma unroll
-            for (int tt = 0; tt < SLICES; ++tt) o[tt] = __shfl_xor_sync(0xffffffffu, w[tt], 16);
-            // B: the W slices, written by the first of each pair once the MMAs
-            // of stage s - 2 (the last to read this buffer) have finished.
-            // (After a failure anywhere, waits are skipped: the result is
-            // poisoned, and the MMA warp waits for its own work before exit.)
-            if (s >= SBUFS && !timed_out && !*abort_flag && !mbar_wait(&b_empty[sb], ((s / SBUFS) - 1) & 1))
-                timed_out = true;
+            // The MMAs of stage s - 1 still read A and, two stages back, B:
+            // wait for them, then write this stage's slices.
+            if (s >= 1 && !mbar_wait(&sl_empty[(s - 1) % SBUFS], ((s - 1) / SBUFS) & 1)) timed_out = true;
+            umma::fence_after_sync();
             unsigned char* bbuf = smem + OFF_B + (size_t)sb * BTILE;
-            if (!vrow) {
-                const uint32_t boff = sw32_offset(j, kq >> 1) + (kq & 1) * 8;
+            const uint32_t boff = sw32_offset(j, kq >> 1) + (kq & 1) * 8;
 #pragma unroll
-                for (int tt = 0; tt < SLICES; ++tt)
-                    *reinterpret_cast<uint2*>(bbuf + boff + tt * (64 * 32)) = make_uint2(w[tt], o[tt]);
+            for (int tt = 0; tt < SLICES; ++tt) {
+                umma::tmem_st2(taddr + lane_base + A_COL + 8 * tt + 2 * kq, w0[tt], w1[tt]);
+                if (!jw) *reinterpret_cast<uint2*>(bbuf + boff + tt * (64 * 32)) = make_uint2(w0[tt], w1[tt]);
             }
+            umma::tmem_wait_st();
             umma::fence_smem_to_async();
+            umma::fence_before_sync();
             if (tid == 0) fresh_flag[sb] = fresh ? 1 : 0;
-            // A, part by part, each once the MMAs of the previous stage that
-            // read that part have finished. V's words keep the Im bytes (1 and
-            // 3) of W's at the Re positions, zeros between.
-#pragma unroll
-            for (int h = 0; h < PARTS; ++h) {
-                if (s >= 1 && !timed_out && !*abort_flag && !mbar_wait(&a_empty[h], (s - 1) & 1)) timed_out = true;
-                __syncwarp();
-                umma::fence_after_sync();
-#pragma unroll
-                for (int tt = part_first(h); tt < part_first(h + 1); ++tt) {
-                    const uint32_t lo = vrow ? __byte_perm(o[tt], 0u, 0x4341) : w[tt];
-                    const uint32_t hi = vrow ? __byte_perm(w[tt], 0u, 0x4341) : o[tt];
-                    umma::tmem_st2(taddr + lane_base + A_COL + 8 * tt + 2 * kq, lo, hi);
-                }
-                umma::tmem_wait_st();
-                umma::fence_before_sync();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&a_full[h]);
-            }
+            mbar_arrive(&sl_full[sb]);
         }
         if (s == nstages && nstages > 0) {
             if (any(!drain(nstages - 1))) fail();
@@ -462,11 +421,11 @@ ozaki_gram_kernel(const __grid_constant__ CUtensorMap tm, int64_t rows, int64_t 
     if (warp == 0) umma::tmem_dealloc(taddr, TMEM_COLS);
 }
 
-// G = alpha (sum over CTAs) + beta C. The partial holds Re G in rows 0-63
-// and P = V^T W in rows 64-127 (stored column n, row m at n * 128 + m):
-// Re G[a][b] = part[b][a], Im G[a][b] = P[b][a] - P[a][b]. Re comes out
-// symmetric to the bit (its slice products are symmetric integers) and Im
-// antisymmetric to the bit, with a zero diagonal.
+// G = alpha (sum over CTAs) + beta C: Re G[a][b] = P[b][a], Im G[a][b] =
+// -P[b][64 + a]. Re comes out symmetric to the bit (its slice products are
+// symmetric integers); Im is made antisymmetric to the bit by taking half the
+// difference of the two mirrored sums, since the slices of -x are not the
+// negated slices of x and so the kept products differ in their last bits.
 __global__ void ozaki_gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int k, int nctas,
                                          const double* __restrict__ partial, const Flags* __restrict__ flags,
                                          z64 alpha, z64 beta, const ChainStatus* st, int gate) {
@@ -475,21 +434,21 @@ __global__ void ozaki_gram_reduce_kernel(z64* __restrict__ C, int64_t ldc, int k
     const int64_t entry = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (entry >= (int64_t)k * k) return;
     const int a = (int)(entry % k), b = (int)(entry / k);
-    double re = 0.0, p_ab = 0.0, p_ba = 0.0;
+    double re = 0.0, im_ab = 0.0, im_ba = 0.0;
     for (int c = lane; c < nctas; c += 32) {
         const double* p = partial + (size_t)c * (128 * 64);
         re += p[(size_t)b * 128 + a];
-        p_ab += p[(size_t)b * 128 + 64 + a];
-        p_ba += p[(size_t)a * 128 + 64 + b];
+        im_ab -= p[(size_t)b * 128 + 64 + a];
+        im_ba -= p[(size_t)a * 128 + 64 + b];
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         re += __shfl_down_sync(0xffffffffu, re, off);
-        p_ab += __shfl_down_sync(0xffffffffu, p_ab, off);
-        p_ba += __shfl_down_sync(0xffffffffu, p_ba, off);
+        im_ab += __shfl_down_sync(0xffffffffu, im_ab, off);
+        im_ba += __shfl_down_sync(0xffffffffu, im_ba, off);
     }
     if (lane != 0) return;
-    double im = a == b ? 0.0 : p_ba - p_ab;
+    double im = a == b ? 0.0 : 0.5 * (im_ab - im_ba);
     if (flags->timeout || flags->nonfinite) re = im = __longlong_as_double(0x7ff8000000000000ll);
     z64 out = zmul(alpha, zmake(re, im));
     z64* dst = C + a + (int64_t)b * ldc;

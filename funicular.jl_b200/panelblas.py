@@ -277,8 +277,10 @@ def cholqr2_streamed(Y: PanelMatrix, *, nbuffers=None, forced_unit_roundoff=None
 def fits_on_device(Y: PanelMatrix) -> bool:
     """Whether the whole matrix, its R and the chain's scratch fit in what the
     plan's device pool has left."""
+    from .plan import device_bytes_to_add
     pool = Y.plan.devicepool
-    need = (Y.N * Y.k + Y.k * Y.k) * Y.dtype.itemsize + kernels.cholqr2_workspace_bytes(Y.N, Y.k)
+    need = (device_bytes_to_add(Y.plan, Y.dtype, [((Y.N, Y.k), 1), ((Y.k, Y.k), 1)])
+            + kernels.cholqr2_workspace_bytes(Y.N, Y.k))
     return pool.allocated + need <= pool.budget
 
 
@@ -381,10 +383,9 @@ def project_schedule(Q: PanelMatrix) -> str:
     gram(Q, Z), src/panelblas.jl:250-261: three crossings of the matrix),
     else the reference's nested schedule (p (p + 1) panel uploads)."""
     from .panels import host_storage_eltype
-    from .plan import host_bytes_in_use
-    nbytes = Q.N * Q.k * Q.dtype.itemsize
+    from .plan import device_bytes_to_add, host_bytes_in_use
     pool = Q.plan.devicepool
-    if pool.allocated + 2 * nbytes + Q.k * Q.k * Q.dtype.itemsize <= pool.budget:
+    if pool.allocated + device_bytes_to_add(Q.plan, Q.dtype, [((Q.N, Q.k), 2), ((Q.k, Q.k), 1)]) <= pool.budget:
         return "resident"
     host_bytes = Q.N * Q.k * np.dtype(host_storage_eltype(Q.plan, Q.dtype)).itemsize
     if Q.plan.hostpool.budget - host_bytes_in_use(Q.plan) >= host_bytes + 64 * Q.npanels():

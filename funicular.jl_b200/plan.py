@@ -211,6 +211,20 @@ def _checkout(plan, dtype, dims, count):
     return out
 
 
+def device_bytes_to_add(plan: ResidencyPlan, dtype, requests) -> int:
+    """Bytes the pool would have to allocate to hand out `requests`, a list of
+    (dims, count): buffers of those dims it already holds, given back by
+    earlier checkouts, cost nothing."""
+    dtype = np.dtype(dtype)
+    pool = plan.devicepool
+    total = 0
+    for dims, count in requests:
+        dims = (int(dims[0]), int(dims[1]))
+        held = len(pool.available[(dtype.str, dims)])
+        total += max(0, int(count) - held) * dims[0] * dims[1] * dtype.itemsize
+    return total
+
+
 def checkin_device_buffers(plan: ResidencyPlan, buffers) -> None:
     """checkin_device_buffers! (src/plan.jl:179-185)."""
     for b in buffers:

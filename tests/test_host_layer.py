@@ -444,6 +444,24 @@ def test_project_matches_panelmul_followed_by_gram(fb, backend, plan, rng):
     assert close(fb.project(Q, dense), fb.gram(Q, Z), blastol(N, k))
 
 
+def test_repeated_calls_keep_their_schedule(fb, backend, make_plan, rng):
+    """The plan's pool keeps the buffers a resident call checked out; a
+    second call of the same shape reuses them and stays resident."""
+    N, k, w = 20_000, 12, 4
+    nbytes = N * k * 16
+    p = make_plan(device_budget=2 * nbytes + 4 * MiB, host_budget=4 * nbytes, panel_width=w)
+    Q = fb.PanelMatrix.from_array(randmatrix(rng, N, k), plan=p)
+    L = fb.Laplacian7((50, 40, 10), 0.5)
+    for _ in range(3):
+        assert fb.panelblas.project_schedule(Q) == "resident"
+        fb.project(Q, L)
+    Y = fb.PanelMatrix.from_array(randmatrix(rng, N, k), plan=make_plan(device_budget=nbytes + 64 * MiB,
+                                                                         host_budget=2 * nbytes, panel_width=w))
+    for _ in range(3):
+        assert fb.panelblas.fits_on_device(Y)
+        fb.cholqr2(Y)
+
+
 def test_project_follows_the_operators_adjoint(fb, backend, plan, rng):
     N, k, w = 40, 23, 7
     G = randmatrix(rng, N, N)

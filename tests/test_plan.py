@@ -147,6 +147,20 @@ def test_device_pool(fb, plan_mod):
         p.checkout_device_buffers(plan, np.complex64, (4, 1), 1)
 
 
+def test_device_bytes_to_add_counts_buffers_the_pool_holds(fb, plan_mod):
+    """A residency check asks what a call would add to the pool: buffers of
+    the right dims given back by an earlier call are reused, not counted
+    again (otherwise a second call of the same shape would take a slower
+    schedule than the first)."""
+    p = plan_mod
+    plan = make_plan(fb, device_budget=10 * 64 * 16)
+    assert p.device_bytes_to_add(plan, C128, [((64, 1), 2), ((4, 4), 1)]) == 2 * 64 * 16 + 16 * 16
+    held = p.checkout_device_buffers(plan, C128, (64, 1), 2)
+    p.checkin_device_buffers(plan, held)
+    assert p.device_bytes_to_add(plan, C128, [((64, 1), 2), ((4, 4), 1)]) == 16 * 16
+    assert p.device_bytes_to_add(plan, C128, [((64, 1), 3)]) == 64 * 16
+
+
 def test_host_pool(fb, plan_mod):
     p = plan_mod
     plan = make_plan(fb, host_budget=4 * 2 ** 20)

@@ -355,13 +355,16 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
 #pragma unroll
             for (int s = 0; s < 4; ++s) ta[s] = reinterpret_cast<const double*>(&buf[tbuf_index(rr, 2 * s + acol)])[apart];
             __syncwarp();
-            // X_b = T_b inv(R_bb)
+            // X_b = T_b inv(R_bb). inv(R_bb) is upper triangular: k-step s
+            // (rows 2s, 2s + 1) meets n-tile t (columns 4t..4t+3) only when
+            // 2s <= 4t + 3, so k-steps 2 and 3 skip n-tile 0.
             double xb[2][2][2] = {};
             const double* fd = frag + pair_index(b, b) * TR_FRAG + lane;
 #pragma unroll
             for (int s = 0; s < 4; ++s)
 #pragma unroll
-                for (int t = 0; t < 2; ++t) dmma_884(xb[s & 1][t][0], xb[s & 1][t][1], ta[s], fd[(s * 2 + t) * 32]);
+                for (int t = 0; t < 2; ++t)
+                    if (2 * s <= 4 * t + 3) dmma_884(xb[s & 1][t][0], xb[s & 1][t][1], ta[s], fd[(s * 2 + t) * 32]);
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 const z64 x = zmake(xb[0][t][0] + xb[1][t][0], xb[0][t][1] + xb[1][t][1]);

@@ -5,10 +5,9 @@
 // x + nx (y + ny z); the 7-point Laplacian has unit spacing and zero
 // (Dirichlet) values outside the grid:
 //   (G v)_p = (6 + shift) v_p - sum of the six neighbours of p.
-// One thread per output entry, x fastest, so the centre, x +- 1 and the
-// store are coalesced 16-byte accesses and the y, z neighbours come from
-// L1/L2 (a plane of a 342^2 grid is 1.9 MB). HBM-bound: 32 bytes per entry
-// (read once, write once) when the neighbours hit in cache.
+// HBM-bound: 32 bytes per entry (read once, write once) when the neighbours
+// are read from DRAM once. Two kernels: by 2.5-D tiles (the default), and a
+// thread per output entry for column counts past the grid limit.
 #include "fb_common.cuh"
 
 namespace fb {
@@ -39,6 +38,58 @@ __global__ void __launch_bounds__(128) laplace7_kernel(z64* __restrict__ Y, int6
                 y[p] = zmake(dr * v.x - di * v.y - s.x, dr * v.y + di * v.x - s.y);
             }
         }
+    }
+}
+
+// The same operator by 2.5-D tiles: a block owns a 32 x 8 tile of an x-y
+// plane of one column and marches it along z. Each thread keeps its point's
+// values at z - 1, z and z + 1 in registers (one new plane read a step), and
+// the x and y neighbours come from the current plane staged in shared memory
+// with a one-point halo (its edge points read from L2, where the neighbouring
+// tiles marching beside this one have brought them). Every input is read
+// from DRAM about once.
+constexpr int LT_X = 32, LT_Y = 8;
+
+__global__ void __launch_bounds__(LT_X * LT_Y)
+laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, int64_t ldx, int nx, int ny,
+                      int nz, z64 shift) {
+    __shared__ z64 tile[LT_Y + 2][LT_X + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int gx = blockIdx.x * LT_X + tx, gy = blockIdx.y * LT_Y + ty;
+    const int c = blockIdx.z;
+    const z64* x = X + (int64_t)c * ldx;
+    z64* y = Y + (int64_t)c * ldy;
+    const int64_t plane = (int64_t)nx * ny;
+    const bool inside = gx < nx && gy < ny;
+    const int64_t col_off = (int64_t)gy * nx + gx;
+    const double dr = 6.0 + shift.x, di = shift.y;
+    const z64 zero = zmake(0.0, 0.0);
+    auto at = [&](int xx, int yy, int zz) -> z64 {
+        return (xx >= 0 && xx < nx && yy >= 0 && yy < ny && zz >= 0 && zz < nz)
+                   ? x[(int64_t)zz * plane + (int64_t)yy * nx + xx] : zero;
+    };
+    z64 below = zero;
+    z64 cur = inside ? x[col_off] : zero;
+    z64 above = (inside && nz > 1) ? x[plane + col_off] : zero;
+    for (int z = 0; z < nz; ++z) {
+        tile[ty + 1][tx + 1] = cur;
+        // Halo: the columns x0 - 1 and x0 + 32 (threads of the first two
+        // warps' lanes 0..7) and the rows y0 - 1 and y0 + 8.
+        if (ty == 0 && tx < LT_Y) tile[tx + 1][0] = at(blockIdx.x * LT_X - 1, blockIdx.y * LT_Y + tx, z);
+        if (ty == 1 && tx < LT_Y) tile[tx + 1][LT_X + 1] = at(blockIdx.x * LT_X + LT_X, blockIdx.y * LT_Y + tx, z);
+        if (ty == 2) tile[0][tx + 1] = at(gx, blockIdx.y * LT_Y - 1, z);
+        if (ty == 3) tile[LT_Y + 1][tx + 1] = at(gx, blockIdx.y * LT_Y + LT_Y, z);
+        __syncthreads();
+        if (inside) {
+            const z64 a = tile[ty + 1][tx], b = tile[ty + 1][tx + 2], d = tile[ty][tx + 1], e = tile[ty + 2][tx + 1];
+            const double sx = a.x + b.x + d.x + e.x + below.x + above.x;
+            const double sy = a.y + b.y + d.y + e.y + below.y + above.y;
+            y[(int64_t)z * plane + col_off] = zmake(dr * cur.x - di * cur.y - sx, dr * cur.y + di * cur.x - sy);
+        }
+        __syncthreads();
+        below = cur;
+        cur = above;
+        above = (inside && z + 2 < nz) ? x[(int64_t)(z + 2) * plane + col_off] : zero;
     }
 }
 
@@ -73,6 +124,13 @@ int fb_zlaplace7_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx, i
         return FB_EINVAL;
     }
     if ((int64_t)ny * nz > INT32_MAX) { set_error(FB_ENOTSUP, "fb_zlaplace7_apply: ny * nz must fit in 32 bits"); return FB_ENOTSUP; }
+    if (cols <= 65535 && (ny + LT_Y - 1) / LT_Y <= 65535) {
+        const dim3 grid((unsigned)((nx + LT_X - 1) / LT_X), (unsigned)((ny + LT_Y - 1) / LT_Y), (unsigned)cols);
+        laplace7_tiled_kernel<<<grid, dim3(LT_X, LT_Y), 0, stream_of(queue)>>>(
+            reinterpret_cast<z64*>(Y), ldy, reinterpret_cast<const z64*>(X), ldx, nx, ny, nz, zmake(shift.re, shift.im));
+        FB_LAUNCHED("laplace7_tiled_kernel");
+        return FB_OK;
+    }
     // Sixteen blocks per SM, every block walking the columns in the same order
     // and the lines of a column in a grid-strided sweep: the lines in flight
     // at one time span a few planes of one column, so the z neighbours of a

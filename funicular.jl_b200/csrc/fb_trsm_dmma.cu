@@ -10,10 +10,12 @@
 // the inverses, and if one exceeds TR_COND_LIMIT the whole CTA solves its rows
 // by plain substitution instead (the reference's ztrsm arithmetic).
 //
-// A warp owns 8 rows at a time for the whole solve, so warps never wait for
-// one another. The solved blocks of its rows stay in registers, already in
-// the MMA A-operand layout; results leave the accumulators (C layout) through
-// a small per-warp shared buffer that transposes them into that layout.
+// A warp owns rows for the whole solve (16 in the blocked path: two 8-row
+// units sharing every B fragment; 8 in the product by the inverse), so warps
+// never wait for one another. The solved blocks of its rows stay in
+// registers, already in the MMA A-operand layout; results leave the
+// accumulators (C layout) through a small per-warp shared buffer that
+// transposes them into that layout.
 // Every CTA first expands R into "fragment order" in shared memory: for each
 // pair of column blocks (c <= b), the 16 x 16 real matrix of the product
 // with -R_cb (c < b) or inv(R_bb) (c = b), laid out so that each lane's MMA B
@@ -269,24 +271,35 @@ trsm_inv_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Trs
     }
 }
 
+// The blocked solve (path blocked) with two adjacent 8-row units a warp (16
+// rows): every B fragment read from shared memory feeds one MMA of each unit,
+// which halves the fragment traffic per MMA against one unit a warp (whose
+// shared pipe and tensor pipe both ran near their limits: 6.91 ms against
+// 6.40 ms at N = 1e7, k = 64), and each warp carries the independent MMA
+// chains of two units. The solved blocks of both units stay in registers (64
+// doubles a lane at k = 64), so a CTA of eight warps runs alone on an SM.
+constexpr int TR2_THREADS = 256;
+
 template <int NBLK>
-__global__ void __launch_bounds__(TR_THREADS, 2)
-trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const TrsmPlan* plan,
-                 const double* __restrict__ gfrag, const ChainStatus* st, int gate) {
+__global__ void __launch_bounds__(TR2_THREADS, 1)
+trsm_dmma2_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const TrsmPlan* plan,
+                  const double* __restrict__ gfrag, const ChainStatus* st, int gate) {
     if (gated_off(st, gate) || plan->path != PATH_BLOCKED) return;
     constexpr int NPAIRS = NBLK * (NBLK + 1) / 2;
+    constexpr int NCH = 4;                   // accumulator chains per unit and n-tile
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* frag = reinterpret_cast<double*>(smem_raw);
     z64* tbuf = reinterpret_cast<z64*>(frag + NPAIRS * TR_FRAG);
     copy_frags(frag, gfrag, NPAIRS * TR_FRAG);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    z64* buf = tbuf + warp * TR_BUF;
+    z64* bufs[2] = {tbuf + (2 * warp) * TR_BUF, tbuf + (2 * warp + 1) * TR_BUF};
     const int rr = lane >> 2;            // row of the 8 this lane's fragments belong to
     const int cq = lane & 3;             // C layout: complex column within a 4-column n-tile
     const int acol = cq >> 1;            // A layout: which of the k-step's two columns
     const int apart = lane & 1;          // A layout: re or im
     const int64_t units = (rows + 7) / 8;
+    const int64_t pairs = (units + 1) / 2;
     const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
 
     // Y of (unit, block) in the C layout, zero past the matrix.
@@ -299,35 +312,38 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
             v[t] = (ok_row && col < k) ? Y[row + (int64_t)col * ldy] : zmake(0.0, 0.0);
         }
     };
-    // The Y blocks of the next two steps are always in flight: a step is one
-    // column block of one unit, and the prefetch runs on into the warp's next
-    // units. Block b of a unit is read from slot b & 1; with an odd block
-    // count the prefetch leaves the next unit's blocks 0 and 1 in slots 1 and
-    // 0, so the slots are swapped at the end of each unit.
-    int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-    z64 yq[2][2];
-    load_y(u, 0, yq[0]);
-    load_y(u + (1 / NBLK) * warps_total, 1 % NBLK, yq[1]);
-    for (; u < units; u += warps_total) {
-        const int64_t row = u * 8 + rr;
-        const bool live = row < rows;
-        z64* yrow = Y + (live ? row : 0);
-        double xa[NBLK][4];
+    // Pair p holds units 2p and 2p + 1. The Y blocks of the next two steps
+    // are always in flight for both units (a step is one column block of the
+    // pair, and the prefetch runs on into the warp's next pairs). Block b is
+    // read from slot b & 1; with an odd block count the prefetch leaves the
+    // next pair's blocks 0 and 1 in slots 1 and 0, so the slots are swapped at
+    // the end of each pair.
+    int64_t pr = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    z64 yq[2][2][2];   // [slot][unit][n-tile]
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+        load_y(2 * pr + v, 0, yq[0][v]);
+        load_y(2 * (pr + (1 / NBLK) * warps_total) + v, 1 % NBLK, yq[1][v]);
+    }
+    for (; pr < pairs; pr += warps_total) {
+        double xa[NBLK][2][4];
 #pragma unroll
         for (int b = 0; b < NBLK; ++b) {
-            constexpr int NCH = 4;                   // accumulator chains per n-tile
-            double acc[NCH][2][2];
+            double acc[2][NCH][2][2];
             const int slot = b & 1;
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                acc[0][t][0] = yq[slot][t].x;
-                acc[0][t][1] = yq[slot][t].y;
+            for (int v = 0; v < 2; ++v)
 #pragma unroll
-                for (int h = 1; h < NCH; ++h) acc[h][t][0] = acc[h][t][1] = 0.0;
-            }
-            // Refill the slot just consumed with the block two steps ahead.
-            load_y(u + ((b + 2) / NBLK) * warps_total, (b + 2) % NBLK, yq[slot]);
-            // Y_b - sum_{c<b} X_c R_cb, k-steps spread over NCH accumulators.
+                for (int t = 0; t < 2; ++t) {
+                    acc[v][0][t][0] = yq[slot][v][t].x;
+                    acc[v][0][t][1] = yq[slot][v][t].y;
+#pragma unroll
+                    for (int h = 1; h < NCH; ++h) acc[v][h][t][0] = acc[v][h][t][1] = 0.0;
+                }
+#pragma unroll
+            for (int v = 0; v < 2; ++v)
+                load_y(2 * (pr + ((b + 2) / NBLK) * warps_total) + v, (b + 2) % NBLK, yq[slot][v]);
+            // Y_b - sum_{c<b} X_c R_cb, each fragment serving both units.
 #pragma unroll
             for (int c = 0; c < b; ++c) {
                 const double* fp = frag + pair_index(c, b) * TR_FRAG + lane;
@@ -335,60 +351,101 @@ trsm_dmma_kernel(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k, const Tr
                 for (int s = 0; s < 4; ++s) {
                     const int h = (c * 4 + s) % NCH;
 #pragma unroll
-                    for (int t = 0; t < 2; ++t)
-                        dmma_884(acc[h][t][0], acc[h][t][1], xa[c][s], fp[(s * 2 + t) * 32]);
+                    for (int t = 0; t < 2; ++t) {
+                        const double bv = fp[(s * 2 + t) * 32];
+                        dmma_884(acc[0][h][t][0], acc[0][h][t][1], xa[c][0][s], bv);
+                        dmma_884(acc[1][h][t][0], acc[1][h][t][1], xa[c][1][s], bv);
+                    }
                 }
             }
             // Transpose T_b from the C layout into the A layout.
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                double re = acc[0][t][0], im = acc[0][t][1];
+            for (int v = 0; v < 2; ++v)
 #pragma unroll
-                for (int h = 1; h < NCH; ++h) {
-                    re += acc[h][t][0];
-                    im += acc[h][t][1];
+                for (int t = 0; t < 2; ++t) {
+                    double re = acc[v][0][t][0], im = acc[v][0][t][1];
+#pragma unroll
+                    for (int h = 1; h < NCH; ++h) {
+                        re += acc[v][h][t][0];
+                        im += acc[v][h][t][1];
+                    }
+                    bufs[v][tbuf_index(rr, 4 * t + cq)] = zmake(re, im);
                 }
-                buf[tbuf_index(rr, 4 * t + cq)] = zmake(re, im);
-            }
             __syncwarp();
-            double ta[4];
+            double ta[2][4];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) ta[s] = reinterpret_cast<const double*>(&buf[tbuf_index(rr, 2 * s + acol)])[apart];
+            for (int v = 0; v < 2; ++v)
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    ta[v][s] = reinterpret_cast<const double*>(&bufs[v][tbuf_index(rr, 2 * s + acol)])[apart];
             __syncwarp();
-            // X_b = T_b inv(R_bb). inv(R_bb) is upper triangular: k-step s
-            // (rows 2s, 2s + 1) meets n-tile t (columns 4t..4t+3) only when
-            // 2s <= 4t + 3, so k-steps 2 and 3 skip n-tile 0.
-            double xb[2][2][2] = {};
+            // X_b = T_b inv(R_bb), inv(R_bb) upper triangular (k-steps 2, 3
+            // skip n-tile 0).
+            double xb[2][2][2][2] = {};
             const double* fd = frag + pair_index(b, b) * TR_FRAG + lane;
 #pragma unroll
             for (int s = 0; s < 4; ++s)
 #pragma unroll
                 for (int t = 0; t < 2; ++t)
-                    if (2 * s <= 4 * t + 3) dmma_884(xb[s & 1][t][0], xb[s & 1][t][1], ta[s], fd[(s * 2 + t) * 32]);
+                    if (2 * s <= 4 * t + 3) {
+                        const double bv = fd[(s * 2 + t) * 32];
+                        dmma_884(xb[0][s & 1][t][0], xb[0][s & 1][t][1], ta[0][s], bv);
+                        dmma_884(xb[1][s & 1][t][0], xb[1][s & 1][t][1], ta[1][s], bv);
+                    }
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                const z64 x = zmake(xb[0][t][0] + xb[1][t][0], xb[0][t][1] + xb[1][t][1]);
-                const int col = TR_NB * b + 4 * t + cq;
-                if (live && col < k) yrow[(int64_t)col * ldy] = x;
-                if (b + 1 < NBLK) buf[tbuf_index(rr, 4 * t + cq)] = x;
+            for (int v = 0; v < 2; ++v) {
+                const int64_t row = (2 * pr + v) * 8 + rr;
+                const bool live = row < rows;
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const z64 x = zmake(xb[v][0][t][0] + xb[v][1][t][0], xb[v][0][t][1] + xb[v][1][t][1]);
+                    const int col = TR_NB * b + 4 * t + cq;
+                    if (live && col < k) Y[row + (int64_t)col * ldy] = x;
+                    if (b + 1 < NBLK) bufs[v][tbuf_index(rr, 4 * t + cq)] = x;
+                }
             }
             if (b + 1 < NBLK) {
                 __syncwarp();
 #pragma unroll
-                for (int s = 0; s < 4; ++s)
-                    xa[b][s] = reinterpret_cast<const double*>(&buf[tbuf_index(rr, 2 * s + acol)])[apart];
+                for (int v = 0; v < 2; ++v)
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+                        xa[b][v][s] = reinterpret_cast<const double*>(&bufs[v][tbuf_index(rr, 2 * s + acol)])[apart];
                 __syncwarp();
             }
         }
         if (NBLK & 1) {
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                const z64 tmp = yq[0][t];
-                yq[0][t] = yq[1][t];
-                yq[1][t] = tmp;
-            }
+            for (int v = 0; v < 2; ++v)
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const z64 tmp = yq[0][v][t];
+                    yq[0][v][t] = yq[1][v][t];
+                    yq[1][v][t] = tmp;
+                }
         }
     }
+}
+
+template <int NBLK>
+static int launch_trsm_dmma2(z64* Y, int64_t ldy, int64_t rows, int k, const TrsmPlan* plan, const double* frag,
+                             cudaStream_t stream, const ChainStatus* st, int gate) {
+    constexpr int NPAIRS = NBLK * (NBLK + 1) / 2;
+    const size_t smem = (size_t)NPAIRS * TR_FRAG * sizeof(double) + (TR2_THREADS / 32) * 2 * TR_BUF * sizeof(z64);
+    FB_CUDA(cudaFuncSetAttribute(trsm_dmma2_kernel<NBLK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "cudaFuncSetAttribute(trsm_dmma2_kernel)");
+    int per_sm = 0;
+    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsm_dmma2_kernel<NBLK>, TR2_THREADS, smem),
+            "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) per_sm = 1;
+    const int64_t pairs = ((rows + 7) / 8 + 1) / 2;
+    int64_t need = (pairs + TR2_THREADS / 32 - 1) / (TR2_THREADS / 32);
+    int64_t grid = (int64_t)sm_count() * per_sm;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    trsm_dmma2_kernel<NBLK><<<(unsigned)grid, TR2_THREADS, smem, stream>>>(Y, ldy, rows, k, plan, frag, st, gate);
+    FB_LAUNCHED("trsm_dmma2_kernel");
+    return FB_OK;
 }
 
 template <int NT>
@@ -411,26 +468,6 @@ static int launch_trsm_inv(z64* Y, int64_t ldy, int64_t rows, int k, const TrsmP
     return FB_OK;
 }
 
-template <int NBLK>
-static int launch_trsm_dmma(z64* Y, int64_t ldy, int64_t rows, int k, const TrsmPlan* plan, const double* frag,
-                            cudaStream_t stream, const ChainStatus* st, int gate) {
-    constexpr int NPAIRS = NBLK * (NBLK + 1) / 2;
-    const size_t smem = (size_t)NPAIRS * TR_FRAG * sizeof(double) + (TR_THREADS / 32) * TR_BUF * sizeof(z64);
-    FB_CUDA(cudaFuncSetAttribute(trsm_dmma_kernel<NBLK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-            "cudaFuncSetAttribute(trsm_dmma_kernel)");
-    int per_sm = 0;
-    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsm_dmma_kernel<NBLK>, TR_THREADS, smem),
-            "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) per_sm = 1;
-    const int64_t units = (rows + 7) / 8;
-    int64_t need = (units + TR_THREADS / 32 - 1) / (TR_THREADS / 32);
-    int64_t grid = (int64_t)sm_count() * per_sm;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    trsm_dmma_kernel<NBLK><<<(unsigned)grid, TR_THREADS, smem, stream>>>(Y, ldy, rows, k, plan, frag, st, gate);
-    FB_LAUNCHED("trsm_dmma_kernel");
-    return FB_OK;
-}
 
 size_t trsm_workspace_bytes_small(int k) {
     return k <= TR_KMAX ? (size_t)TR_PLAN_BYTES + (size_t)TR_FRAG_DOUBLES * sizeof(double) : 0;
@@ -463,7 +500,7 @@ int trsm_dmma_enqueue(z64* Y, int64_t ldy, int64_t rows, int k, const z64* R, in
     }
     FB_TRY(status);
     switch ((k + TR_NB - 1) / TR_NB) {
-#define FB_BLK_CASE(n) case n: status = launch_trsm_dmma<n>(Y, ldy, rows, k, plan, frag, stream, st, gate); break;
+#define FB_BLK_CASE(n) case n: status = launch_trsm_dmma2<n>(Y, ldy, rows, k, plan, frag, stream, st, gate); break;
         FB_BLK_CASE(1) FB_BLK_CASE(2) FB_BLK_CASE(3) FB_BLK_CASE(4)
         FB_BLK_CASE(5) FB_BLK_CASE(6) FB_BLK_CASE(7) FB_BLK_CASE(8)
 #undef FB_BLK_CASE

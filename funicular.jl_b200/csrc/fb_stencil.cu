@@ -42,21 +42,25 @@ __global__ void __launch_bounds__(128) laplace7_kernel(z64* __restrict__ Y, int6
 }
 
 // The same operator by 2.5-D tiles: a block owns a 32 x 8 tile of an x-y
-// plane of one column and marches it along z. Each thread keeps its point's
-// values at z - 1, z and z + 1 in registers (one new plane read a step), and
-// the x and y neighbours come from the current plane staged in shared memory
-// with a one-point halo (its edge points read from L2, where the neighbouring
-// tiles marching beside this one have brought them). Every input is read
-// from DRAM about once.
+// plane of one column and marches it along a range of z. Each thread keeps
+// its point's values at z - 1, z and z + 1 in registers, with the plane at
+// z + 2 already loading (one new plane read a step, two steps ahead of its
+// use), and the x and y neighbours come from the current plane staged in
+// shared memory with a one-point halo (its edge points read from L2, where
+// the neighbouring tiles marching beside this one have brought them). Every
+// input is read from DRAM about once. The z range of a column is cut into
+// zchunks pieces, enough for the grid to fill the GPU when there are few
+// columns.
 constexpr int LT_X = 32, LT_Y = 8;
 
 __global__ void __launch_bounds__(LT_X * LT_Y)
 laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, int64_t ldx, int nx, int ny,
-                      int nz, z64 shift) {
+                      int nz, z64 shift, int zchunks) {
     __shared__ z64 tile[LT_Y + 2][LT_X + 2];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int gx = blockIdx.x * LT_X + tx, gy = blockIdx.y * LT_Y + ty;
-    const int c = blockIdx.z;
+    const int c = blockIdx.z / zchunks, zc = blockIdx.z - c * zchunks;
+    const int z0 = (int)((int64_t)nz * zc / zchunks), z1 = (int)((int64_t)nz * (zc + 1) / zchunks);
     const z64* x = X + (int64_t)c * ldx;
     z64* y = Y + (int64_t)c * ldy;
     const int64_t plane = (int64_t)nx * ny;
@@ -68,10 +72,12 @@ laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ 
         return (xx >= 0 && xx < nx && yy >= 0 && yy < ny && zz >= 0 && zz < nz)
                    ? x[(int64_t)zz * plane + (int64_t)yy * nx + xx] : zero;
     };
-    z64 below = zero;
-    z64 cur = inside ? x[col_off] : zero;
-    z64 above = (inside && nz > 1) ? x[plane + col_off] : zero;
-    for (int z = 0; z < nz; ++z) {
+    auto plane_at = [&](int zz) -> z64 { return (inside && zz >= 0 && zz < nz) ? x[(int64_t)zz * plane + col_off] : zero; };
+    z64 below = plane_at(z0 - 1);
+    z64 cur = plane_at(z0);
+    z64 above = plane_at(z0 + 1);
+    z64 ahead = plane_at(z0 + 2);
+    for (int z = z0; z < z1; ++z) {
         tile[ty + 1][tx + 1] = cur;
         // Halo: the columns x0 - 1 and x0 + 32 (threads of the first two
         // warps' lanes 0..7) and the rows y0 - 1 and y0 + 8.
@@ -89,7 +95,8 @@ laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ 
         __syncthreads();
         below = cur;
         cur = above;
-        above = (inside && z + 2 < nz) ? x[(int64_t)(z + 2) * plane + col_off] : zero;
+        above = ahead;
+        ahead = plane_at(z + 3);
     }
 }
 
@@ -124,10 +131,17 @@ int fb_zlaplace7_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx, i
         return FB_EINVAL;
     }
     if ((int64_t)ny * nz > INT32_MAX) { set_error(FB_ENOTSUP, "fb_zlaplace7_apply: ny * nz must fit in 32 bits"); return FB_ENOTSUP; }
-    if (cols <= 65535 && (ny + LT_Y - 1) / LT_Y <= 65535) {
-        const dim3 grid((unsigned)((nx + LT_X - 1) / LT_X), (unsigned)((ny + LT_Y - 1) / LT_Y), (unsigned)cols);
+    const int64_t tiles = (int64_t)((nx + LT_X - 1) / LT_X) * ((ny + LT_Y - 1) / LT_Y);
+    // z pieces: enough blocks for eight a SM, each piece at least 16 planes.
+    int64_t zchunks = ((int64_t)sm_count() * 8 + tiles * cols - 1) / (tiles * cols);
+    if (zchunks > nz / 16) zchunks = nz / 16;
+    if (zchunks < 1) zchunks = 1;
+    if (cols * zchunks <= 65535 && (ny + LT_Y - 1) / LT_Y <= 65535) {
+        const dim3 grid((unsigned)((nx + LT_X - 1) / LT_X), (unsigned)((ny + LT_Y - 1) / LT_Y),
+                        (unsigned)(cols * zchunks));
         laplace7_tiled_kernel<<<grid, dim3(LT_X, LT_Y), 0, stream_of(queue)>>>(
-            reinterpret_cast<z64*>(Y), ldy, reinterpret_cast<const z64*>(X), ldx, nx, ny, nz, zmake(shift.re, shift.im));
+            reinterpret_cast<z64*>(Y), ldy, reinterpret_cast<const z64*>(X), ldx, nx, ny, nz, zmake(shift.re, shift.im),
+            (int)zchunks);
         FB_LAUNCHED("laplace7_tiled_kernel");
         return FB_OK;
     }

@@ -77,14 +77,19 @@ laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ 
     z64 cur = plane_at(z0);
     z64 above = plane_at(z0 + 1);
     z64 ahead = plane_at(z0 + 2);
+    // Halo: the columns x0 - 1 and x0 + 32 (lanes 0..7 of the first two
+    // warps) and the rows y0 - 1 and y0 + 8 (the next two warps); each such
+    // thread loads its halo point one plane ahead.
+    int hx = -2, hy = -2, hr = 0, hc = 0;
+    if (ty == 0 && tx < LT_Y) { hx = blockIdx.x * LT_X - 1; hy = blockIdx.y * LT_Y + tx; hr = tx + 1; hc = 0; }
+    if (ty == 1 && tx < LT_Y) { hx = blockIdx.x * LT_X + LT_X; hy = blockIdx.y * LT_Y + tx; hr = tx + 1; hc = LT_X + 1; }
+    if (ty == 2) { hx = gx; hy = blockIdx.y * LT_Y - 1; hr = 0; hc = tx + 1; }
+    if (ty == 3) { hx = gx; hy = blockIdx.y * LT_Y + LT_Y; hr = LT_Y + 1; hc = tx + 1; }
+    const bool halo = hx != -2;
+    z64 hval = halo ? at(hx, hy, z0) : zero;
     for (int z = z0; z < z1; ++z) {
         tile[ty + 1][tx + 1] = cur;
-        // Halo: the columns x0 - 1 and x0 + 32 (threads of the first two
-        // warps' lanes 0..7) and the rows y0 - 1 and y0 + 8.
-        if (ty == 0 && tx < LT_Y) tile[tx + 1][0] = at(blockIdx.x * LT_X - 1, blockIdx.y * LT_Y + tx, z);
-        if (ty == 1 && tx < LT_Y) tile[tx + 1][LT_X + 1] = at(blockIdx.x * LT_X + LT_X, blockIdx.y * LT_Y + tx, z);
-        if (ty == 2) tile[0][tx + 1] = at(gx, blockIdx.y * LT_Y - 1, z);
-        if (ty == 3) tile[LT_Y + 1][tx + 1] = at(gx, blockIdx.y * LT_Y + LT_Y, z);
+        if (halo) tile[hr][hc] = hval;
         __syncthreads();
         if (inside) {
             const z64 a = tile[ty + 1][tx], b = tile[ty + 1][tx + 2], d = tile[ty][tx + 1], e = tile[ty + 2][tx + 1];
@@ -97,6 +102,7 @@ laplace7_tiled_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ 
         cur = above;
         above = ahead;
         ahead = plane_at(z + 3);
+        if (halo) hval = at(hx, hy, z + 1);
     }
 }
 

@@ -282,37 +282,37 @@ class ClockSampler:
 def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier, hbm_peak, fp64_peak):
     """The batched range finder's orthonormalization: args.batch independent
     cholqr2! instances, N log-uniform on [1e4, 2e6], k drawn from {16, 32, 64}
-    (seeded), all enqueued by one fb_zcholqr2_batched call, timed eagerly and
-    as one captured CUDA graph. Inputs are seeded complex Gaussians; each step
-    orthonormalizes in place (the later steps see orthonormal columns, which
-    moves the same bytes through the same kernels)."""
+    (seeded), on both batch schedules: the persistent kernel (the whole batch
+    as one launch) and the eight stream lanes, each timed eagerly and as one
+    captured CUDA graph, then the lanes again after the autotuner. Inputs are
+    seeded complex Gaussians, refilled before each schedule's checked run;
+    the timed steps orthonormalize in place (the later steps see orthonormal
+    columns, which moves the same bytes through the same kernels)."""
     rng = np.random.default_rng(0xBA7C4)
     count = args.batch
     Ns = np.exp(rng.uniform(np.log(1e4), np.log(2e6), count)).astype(np.int64)
     ks = rng.choice([16, 32, 64], count)
-    gen = torch.Generator(device=device)
-    gen.manual_seed(0xBA7C4)
-    tensors = [torch.randn((int(k), int(N)), dtype=torch.complex128, device=device, generator=gen)
-               for N, k in zip(Ns, ks)]
-    torch.cuda.synchronize()
+    tensors = [torch.empty((int(k), int(N)), dtype=torch.complex128, device=device) for N, k in zip(Ns, ks)]
+
+    def refill():
+        gen = torch.Generator(device=device)
+        gen.manual_seed(0xBA7C4)
+        for t in tensors:
+            t.copy_(torch.randn(t.shape, dtype=torch.complex128, device=device, generator=gen))
+        torch.cuda.synchronize()
+
     Ys = [wrap(fb, t, int(N), int(k)) for t, N, k in zip(tensors, Ns, ks)]
     Rs = [backend.alloc_device(np.complex128, (int(k), int(k))) for k in ks]
-    nbytes = fb.kernels.cholqr2_batched_workspace_bytes([(int(N), int(k)) for N, k in zip(Ns, ks)])
-    ws_buf = backend.alloc_device(np.complex128, (nbytes // 16 + 32, 1))
-    ws = ((ws_buf.ptr + 255) // 256 * 256, nbytes)
+    shapes = [(int(N), int(k)) for N, k in zip(Ns, ks)]
     queue = backend.make_queue()
     stream = torch.cuda.ExternalStream(queue.handle, device=device)
-    # Checked run: passes and the worst orthogonality over the instances.
-    passes = []
-    backend.submit(queue, lambda: passes.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws)))
-    worst = 0.0
-    for t in tensors:
-        Q = t.t()
-        worst = max(worst, float(torch.linalg.matrix_norm(Q.conj().t() @ Q
-                                                          - torch.eye(Q.shape[1], dtype=Q.dtype, device=device))))
-    eager = lambda: backend.submit(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False,
-                                                                            workspace=ws))
-    graph = backend.capture(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws))
+    keep = []
+
+    def workspace(schedule):
+        nbytes = fb.kernels.cholqr2_batched_workspace_bytes(shapes, schedule=schedule)
+        buf = backend.alloc_device(np.complex128, (nbytes // 16 + 32, 1))
+        keep.append(buf)
+        return ((buf.ptr + 255) // 256 * 256, nbytes)
 
     def timed(step):
         for _ in range(max(1, args.warmup)):
@@ -328,42 +328,65 @@ def run_batched(args, fb, backend, torch, device, world, max_over_ranks, barrier
         b.synchronize()
         return max_over_ranks(a.elapsed_time(b) / args.steps)
 
-    ms_eager = timed(eager)
-    ms_graph = timed(lambda: graph.launch(queue))
     alg = float(sum(96.0 * N * k for N, k in zip(Ns, ks)))
     # The batch's roofline: each instance at the slower of its HBM time
     # (96 N k bytes) and its FP64 time (16 N k^2 flops), summed.
     roof_ms = float(sum(max(96.0 * N * k / (hbm_peak * 1e9), 16.0 * N * k * k / (fp64_peak * 1e12))
                         for N, k in zip(Ns, ks))) * 1e3
-    del graph
-    # The same batch after the autotuner has chosen the Gram's row chunks for
-    # each shape class of the batch (each class tuned at its largest N).
-    shapes = [(int(N), int(k)) for N, k in zip(Ns, ks)]
+    out = {}
+    for schedule in ("persistent", "lanes"):
+        ws = workspace(schedule)
+        refill()
+        passes = []
+        backend.submit(queue, lambda: passes.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws,
+                                                                                schedule=schedule)))
+        worst = 0.0
+        for t in tensors:
+            Q = t.t()
+            worst = max(worst, float(torch.linalg.matrix_norm(Q.conj().t() @ Q - torch.eye(
+                Q.shape[1], dtype=Q.dtype, device=device))))
+        enqueue = lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws, schedule=schedule)
+        ms_eager = timed(lambda: backend.submit(queue, enqueue))
+        graph = backend.capture(queue, enqueue)
+        ms_graph = timed(lambda: graph.launch(queue))
+        del graph
+        out[schedule] = {"ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
+                         "value_graph": whole_job_gbs(alg, world, ms_graph),
+                         "value_eager": whole_job_gbs(alg, world, ms_eager),
+                         "roofline_frac_graph": roof_ms / ms_graph, "passes_max": max(passes),
+                         "orthogonality_fro_max": worst}
+    out["persistent"]["launch"] = ("fb_zcholqr2_batched_persistent: a memset and one persistent kernel launch "
+                                   "(one CTA per SM taking Gram, factor and solve jobs from a ticket counter)")
+    out["lanes"]["launch"] = "fb_zcholqr2_batched: each instance's chain on one of eight stream lanes"
+    # The lanes after the autotuner has chosen the Gram's row chunks for each
+    # shape class of the batch (each class tuned at its largest N) and the
+    # lane count.
     t0 = time.perf_counter()
     tuned = fb.autotune.tune_shapes(backend, shapes, forms=False)
     lanes = fb.autotune.tune_batch_lanes(backend, Ys, Rs)
     tune_s = time.perf_counter() - t0
-    nbytes_t = fb.kernels.cholqr2_batched_workspace_bytes(shapes)
-    ws_buf_t = backend.alloc_device(np.complex128, (nbytes_t // 16 + 32, 1))
-    ws_t = ((ws_buf_t.ptr + 255) // 256 * 256, nbytes_t)
-    graph_t = backend.capture(queue, lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws_t))
+    ws_t = workspace("lanes")
+    enqueue_t = lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws_t, schedule="lanes")
+    graph_t = backend.capture(queue, enqueue_t)
     ms_tuned = timed(lambda: graph_t.launch(queue))
     passes_t = []
-    backend.submit(queue, lambda: passes_t.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws_t)))
+    backend.submit(queue, lambda: passes_t.extend(fb.kernels.cholqr2_batched(backend, Ys, Rs, workspace=ws_t,
+                                                                              schedule="lanes")))
     shifts = sorted({r["gram_shift"] for r in tuned})
     fb.autotune.clear()
     del graph_t, tensors, Ys
+    out["lanes"]["tuned"] = {"ms_per_step_graph": ms_tuned, "value_graph": whole_job_gbs(alg, world, ms_tuned),
+                             "shape_classes": len(tuned), "gram_shifts_chosen": shifts, "lanes": lanes["lanes"],
+                             "ms_by_lanes_eager": lanes["ms"], "tuning_s": tune_s, "passes_max": max(passes_t)}
+    p = out["persistent"]
     return {"instances": count, "N_range": [int(Ns.min()), int(Ns.max())], "k_values": [16, 32, 64],
-            "tuned": {"ms_per_step_graph": ms_tuned, "value_graph": whole_job_gbs(alg, world, ms_tuned),
-                      "shape_classes": len(tuned), "gram_shifts_chosen": shifts, "lanes": lanes["lanes"],
-                      "ms_by_lanes_eager": lanes["ms"], "tuning_s": tune_s,
-                      "passes_max": max(passes_t)},
-            "alg_bytes_per_step": alg, "ms_per_step_eager": ms_eager, "ms_per_step_graph": ms_graph,
-            "roofline": {"ms": roof_ms, "frac_graph": roof_ms / ms_graph, "frac_eager": roof_ms / ms_eager,
+            "alg_bytes_per_step": alg, "ms_per_step_graph": p["ms_per_step_graph"],
+            "ms_per_step_eager": p["ms_per_step_eager"], "value_graph": p["value_graph"],
+            "value_eager": p["value_eager"], "unit": UNIT, "schedule": "persistent",
+            "roofline": {"ms": roof_ms, "frac_graph": roof_ms / p["ms_per_step_graph"],
+                         "frac_eager": roof_ms / p["ms_per_step_eager"],
                          "rule": "sum over instances of max(96 N k / HBM peak, 16 N k^2 / FP64 peak)"},
-            "value_graph": whole_job_gbs(alg, world, ms_graph), "value_eager": whole_job_gbs(alg, world, ms_eager),
-            "unit": UNIT, "passes_max": max(passes), "orthogonality_fro_max": worst,
-            "launch": "one fb_zcholqr2_batched call (eight stream lanes), replayed as one captured CUDA graph"}
+            "persistent": out["persistent"], "lanes": out["lanes"]}
 
 
 C1_K, C1_W, C1_SEED = 32, 8, 0xDEADBEEF

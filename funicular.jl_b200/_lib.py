@@ -119,6 +119,8 @@ SIGNATURES = {
     "fb_zcholqr2_batched_workspace_size": [_vp, _vp, _int, _psz],
     "fb_zcholqr2_batched": [_vp, _vp, _vp, _vp, _vp, _vp, _int, _int, _vp, _sz, _vp],
     "fb_zcholqr2_batched_query": [_vp, _int, _vp, _vp],
+    "fb_zcholqr2_batched_persistent_workspace_size": [_vp, _vp, _int, _psz],
+    "fb_zcholqr2_batched_persistent": [_vp, _vp, _vp, _vp, _vp, _vp, _int, _vp, _sz, _vp],
     "fb_ghost_fill": [_vp, _int, _i64, _i64, _i64, _i64, _i64, ctypes.c_uint64, _int, _vp],
     "fb_zcholqr2_adjoint_workspace_size": [_i64, _int, _psz],
     "fb_zcholqr2_adjoint": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _int, _vp, _sz, _vp],

@@ -145,7 +145,7 @@ def tune_batch_lanes(backend, Ys, Rs, *, reps: int = 3) -> dict:
     ms = {}
     for lanes in BATCH_LANES:
         set_batch_lanes(lanes)
-        ms[lanes] = _time(backend, lambda: kernels.cholqr2_batched(backend, Ys, Rs, wait=False), reps)
+        ms[lanes] = _time(backend, lambda: kernels.cholqr2_batched(backend, Ys, Rs, wait=False, schedule="lanes"), reps)
     best = min(ms, key=ms.get)
     if ms[best] > 0.97 * ms[8]:
         best = 8

@@ -330,6 +330,11 @@ int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shi
     if (!workspace) { set_error(FB_EINVAL, "fb_zcholqr2_query: NULL workspace"); return FB_EINVAL; }
     ChainStatus host{};
     FB_CUDA(cudaMemcpy(&host, workspace, sizeof host, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (host.timeout) {
+        set_error(FB_ECUDA, "cholqr2! batch: a device-side wait of the persistent kernel gave up after its 2 s "
+                  "limit, so the results are not valid");
+        return FB_ECUDA;
+    }
     if (info) *info = host.failed;
     if (passes) *passes = (host.shifted[1] | host.shifted[2]) ? 3 : 2;
     if (shifts)

@@ -14,32 +14,12 @@
 // unit roundoff u > 0 the kernel factors G + s I once, s = 11 (N k + k (k+1))
 // u ||G||_F (||G||_F bounds ||Y||_2^2 from above, which keeps s inside the
 // range the analysis allows for the condition numbers it targets).
-#include "fb_common.cuh"
+#include "fb_factor.cuh"
 
 namespace fb {
 
 constexpr int POTRF_THREADS = 512;
 constexpr int POTRF_SMEM_MAX_K = 112;
-
-__device__ double block_sum(double v, double* scratch) {
-    // Fixed-order reduction: warp shuffle tree, then warp 0 over the warps.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    __syncthreads();
-    if (lane == 0) scratch[warp] = v;
-    __syncthreads();
-    double total = 0.0;
-    if (warp == 0) {
-        double w = lane < nwarps ? scratch[lane] : 0.0;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) w += __shfl_down_sync(0xffffffffu, w, off);
-        if (lane == 0) scratch[32] = w;
-    }
-    __syncthreads();
-    total = scratch[32];
-    return total;
-}
 
 __global__ void __launch_bounds__(POTRF_THREADS, 1)
 potrf_kernel(const z64* __restrict__ G, int64_t ldg, int k, int64_t N,
@@ -53,75 +33,11 @@ potrf_kernel(const z64* __restrict__ G, int64_t ldg, int k, int64_t N,
     z64* W = in_smem ? reinterpret_cast<z64*>(smem_raw) : gwork;  // row-major k x k, upper part used
     const int tid = threadIdx.x, nt = blockDim.x;
     const int kk = k * k;
-
-    // ||G||_F over the full Hermitian matrix the upper triangle stands for.
-    double part = 0.0;
-    for (int e = tid; e < kk; e += nt) {
-        int i = e / k, j = e - i * k;
-        if (i <= j) {
-            z64 g = G[i + (int64_t)j * ldg];
-            double a2 = fma(g.x, g.x, g.y * g.y);
-            part += (i == j) ? a2 : 2.0 * a2;
-        }
-    }
-    const double gnorm = sqrt(block_sum(part, red_scratch));
-
+    auto g = [&](int i, int j) { return G[i + (int64_t)j * ldg]; };
+    const double gnorm = hermitian_fro(g, k, red_scratch);
     bool shifted = false;
     double shift = 0.0;
-    bool ok = false;
-    if (forced_u > 0.0) {
-        shifted = true;
-        shift = 11.0 * ((double)N * (double)k + (double)k * (double)(k + 1)) * forced_u * gnorm;
-    }
-    const int attempts = forced_u > 0.0 ? 1 : 2;
-    for (int attempt = 0; attempt < attempts && !ok; ++attempt) {
-        if (attempt == 1) {
-            shifted = true;
-            shift = 11.0 * (double)N * (double)k * 2.220446049250313e-16 * gnorm;
-        }
-        __syncthreads();
-        for (int e = tid; e < kk; e += nt) {
-            int i = e / k, j = e - i * k;
-            z64 v = zmake(0.0, 0.0);
-            if (i <= j) {
-                v = G[i + (int64_t)j * ldg];
-                if (i == j) v = zmake(v.x + shift, 0.0);
-            }
-            W[e] = v;
-        }
-        ok = true;
-        for (int j = 0; j < k; ++j) {
-            __syncthreads();
-            const double d = W[j * k + j].x;
-            if (!(d > 0.0)) { ok = false; break; }
-            const double rj = sqrt(d);
-            const double inv = 1.0 / rj;
-            for (int l = j + 1 + tid; l < k; l += nt) {
-                z64 v = W[j * k + l];
-                W[j * k + l] = zmake(v.x * inv, v.y * inv);
-            }
-            __syncthreads();
-            if (tid == 0) W[j * k + j] = zmake(rj, 0.0);
-            // The trailing upper triangle: a warp per row m, its lanes along
-            // the row's columns l >= m (each entry updated once per step, so
-            // the order across entries does not reach the bits).
-            const int warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
-            for (int m = j + 1 + warp; m < k; m += nwarps) {
-                const z64 a = W[j * k + m];
-                for (int l = m + lane; l < k; l += 32) {
-                    const z64 b = W[j * k + l];
-                    z64 w = W[m * k + l];
-                    // w -= conj(a) * b
-                    w.x = fma(-a.x, b.x, w.x);
-                    w.x = fma(-a.y, b.y, w.x);
-                    w.y = fma(-a.x, b.y, w.y);
-                    w.y = fma(a.y, b.x, w.y);
-                    W[m * k + l] = w;
-                }
-            }
-        }
-        __syncthreads();
-    }
+    const bool ok = factor_shifted(g, k, N, gnorm, forced_u, W, shifted, shift);
 
     if (tid == 0 && st) {
         st->shifted[pass] = shifted ? 1 : 0;

@@ -20,38 +20,12 @@
 // pair of column blocks (c <= b), the 16 x 16 real matrix of the product
 // with -R_cb (c < b) or inv(R_bb) (c = b), laid out so that each lane's MMA B
 // operand is one consecutive 8-byte load.
-#include "fb_common.cuh"
+#include "fb_factor.cuh"
 #include "fb_tma.cuh"
 
 namespace fb {
 
-constexpr int TR_NB = 8;                 // complex columns per block
-constexpr int TR_FRAG = 256;             // doubles per block pair: 4 k-steps x 2 n-tiles x 32 lanes
-constexpr double TR_COND_LIMIT = 1.0e4;  // cond_1 of a diagonal block above which substitution is used
 constexpr int TR_THREADS = 256;
-constexpr int TR_BUF = TR_NB * TR_NB;    // per-warp transpose buffer: 8 rows x 8 complex, swizzled
-
-// Where (row, col) of the 8 x 8 transpose buffer lives. The writes (C layout:
-// a quarter warp covers rows 2j, 2j+1 and four consecutive columns) and the
-// reads (A layout: a half warp covers rows 4j..4j+3 and two columns) both
-// touch eight different 16-byte chunks of a 128-byte line this way.
-__device__ __forceinline__ int tbuf_index(int row, int col) {
-    return row * TR_NB + ((col + 4 * (row & 1) + 2 * ((row >> 1) & 1)) & 7);
-}
-
-__device__ __forceinline__ int pair_index(int c, int b) { return b * (b + 1) / 2 + c; }
-
-// Entry (kr, nr) of the real 16 x 16 form of a complex 8 x 8 block M:
-// kr = 2 i + p (row i of M, part p of the X entry it multiplies),
-// nr = 2 j + o (column j of M, part o of the output).
-__device__ __forceinline__ double real_form(z64 m, int p, int o) {
-    return o == 0 ? (p == 0 ? m.x : -m.y) : (p == 0 ? m.y : m.x);
-}
-
-__device__ __forceinline__ z64 zrecip_d(z64 d) {
-    double s = 1.0 / fma(d.x, d.x, d.y * d.y);
-    return zmake(d.x * s, -d.y * s);
-}
 
 // Substitution for rows in [first, rows) step `stride`: the fallback.
 __device__ void trsm_substitute_rows(z64* __restrict__ Y, int64_t ldy, int64_t rows, int k,
@@ -66,20 +40,6 @@ __device__ void trsm_substitute_rows(z64* __restrict__ Y, int64_t ldy, int64_t r
     }
 }
 
-constexpr double TR_INV_COND_LIMIT = 16.0;  // cond_1(R) up to which Y R^-1 is one product by inv(R)
-constexpr int TR_KMAX = 64;
-constexpr int TR_PLAN_BYTES = 256;
-constexpr int TR_FRAG_DOUBLES = 36 * TR_FRAG;   // the larger of the two fragment sets at k = 64
-
-enum TrsmPath : int { PATH_INVERSE = 0, PATH_BLOCKED = 1, PATH_SUBSTITUTE = 2 };
-
-struct TrsmPlan {
-    int path;
-    int pad;
-    double cond;          // cond_1(R)
-    double cond_blocks;   // largest cond_1 of an 8 x 8 diagonal block
-};
-
 // One CTA: inv(R) in shared memory, the condition numbers, the choice of
 // path, and the chosen path's B fragments in the workspace.
 //   inverse:    cond_1(R) <= TR_INV_COND_LIMIT: Y inv(R) as one product
@@ -93,13 +53,10 @@ __global__ void __launch_bounds__(256, 1)
 trsm_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, TrsmPlan* plan, double* __restrict__ frag,
                  const ChainStatus* st, int gate) {
     if (gated_off(st, gate)) return;
-    constexpr int LD = TR_KMAX + 1;
+    constexpr int LD = TR_PREP_LD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     z64* Rs = reinterpret_cast<z64*>(smem_raw);   // KP x KP, padded with the identity
     z64* Xs = Rs + TR_KMAX * LD;                   // inv(R)
-    __shared__ z64 dinv[TR_KMAX];
-    __shared__ double colr[TR_KMAX], coli[TR_KMAX];
-    __shared__ int path;
     const int tid = threadIdx.x;
     const int KP = (k + TR_NB - 1) / TR_NB * TR_NB;
     for (int e = tid; e < KP * KP; e += blockDim.x) {
@@ -110,95 +67,7 @@ trsm_prep_kernel(const z64* __restrict__ R, int64_t ldr, int k, TrsmPlan* plan, 
         Xs[i * LD + j] = zmake(0.0, 0.0);
     }
     __syncthreads();
-    for (int j = tid; j < KP; j += blockDim.x) dinv[j] = zrecip_d(Rs[j * LD + j]);
-    __syncthreads();
-    // Row i of inv(R): X[i][j] = (delta_ij - sum_{i<l<=j} R[i][l] X[l][j]) / R[i][i].
-    const int col = tid >> 2, part = tid & 3;
-    for (int i = KP - 1; i >= 0; --i) {
-        z64 acc = zmake(0.0, 0.0);
-        if (col < KP && col >= i)
-            for (int l = i + 1 + part; l <= col; l += 4) zmac(acc, Rs[i * LD + l], Xs[l * LD + col]);
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
-        if (col < KP && col >= i && part == 0) {
-            const z64 rhs = zmake((i == col ? 1.0 : 0.0) - acc.x, -acc.y);
-            Xs[i * LD + col] = zmul(rhs, dinv[i]);
-        }
-        __syncthreads();
-    }
-    // 1-norms of R's own columns and of inv(R)'s, and of the columns of
-    // their 8 x 8 diagonal blocks: a thread per column, each sum in row order.
-    __shared__ double bcolr[TR_KMAX], bcoli[TR_KMAX];
-    if (tid < KP) {
-        double a = 0.0, b = 0.0;
-        for (int i = 0; i <= tid; ++i) {
-            a += hypot(Rs[i * LD + tid].x, Rs[i * LD + tid].y);
-            b += hypot(Xs[i * LD + tid].x, Xs[i * LD + tid].y);
-        }
-        colr[tid] = tid < k ? a : 0.0;
-        coli[tid] = tid < k ? b : 0.0;
-        double cr = 0.0, ci = 0.0;
-        for (int i = TR_NB * (tid / TR_NB); i <= tid; ++i) {
-            cr += hypot(Rs[i * LD + tid].x, Rs[i * LD + tid].y);
-            ci += hypot(Xs[i * LD + tid].x, Xs[i * LD + tid].y);
-        }
-        bcolr[tid] = cr;
-        bcoli[tid] = ci;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double nr = 0.0, ni = 0.0;
-        for (int j = 0; j < KP; ++j) {
-            nr = fmax(nr, colr[j]);
-            ni = fmax(ni, coli[j]);
-        }
-        const double cond = nr * ni;
-        double worst = 0.0;
-        for (int b = 0; b < KP / TR_NB; ++b) {
-            double br = 0.0, bi = 0.0;
-            for (int j = TR_NB * b; j < TR_NB * b + TR_NB; ++j) {
-                br = fmax(br, bcolr[j]);
-                bi = fmax(bi, bcoli[j]);
-            }
-            worst = fmax(worst, br * bi);
-        }
-        int p = PATH_SUBSTITUTE;
-        if (cond <= TR_INV_COND_LIMIT) p = PATH_INVERSE;
-        else if (worst <= TR_COND_LIMIT) p = PATH_BLOCKED;
-        path = p;
-        plan->path = p;
-        plan->cond = cond;
-        plan->cond_blocks = worst;
-    }
-    __syncthreads();
-    if (path == PATH_INVERSE) {
-        const int NT = (k + 3) / 4;
-        for (int e = tid; e < 32 * NT * (NT + 1); e += blockDim.x) {
-            int t = 0;
-            while (32 * (t + 1) * (t + 2) <= e) ++t;
-            const int f = e - 32 * t * (t + 1);
-            const int s = f >> 5, lane = f & 31;
-            const int i = 2 * s + ((lane & 3) >> 1), p = lane & 1;
-            const int j = 4 * t + ((lane >> 2) >> 1), o = (lane >> 2) & 1;
-            frag[e] = (i <= j) ? real_form(Xs[i * LD + j], p, o) : 0.0;
-        }
-    } else if (path == PATH_BLOCKED) {
-        const int NBLK = KP / TR_NB;
-        const int npairs = NBLK * (NBLK + 1) / 2;
-        for (int e = tid; e < npairs * TR_FRAG; e += blockDim.x) {
-            const int pr = e / TR_FRAG, f = e - pr * TR_FRAG;
-            int b = 0;
-            while (pair_index(0, b + 1) <= pr) ++b;
-            const int c = pr - pair_index(0, b);
-            const int lane = f & 31, st_ = f >> 5, s = st_ >> 1, t = st_ & 1;
-            const int kr = 4 * s + (lane & 3), nr = 8 * t + (lane >> 2);
-            const int i = TR_NB * c + (kr >> 1), p = kr & 1, j = TR_NB * b + (nr >> 1), o = nr & 1;
-            // -R_cb off the diagonal; inv(R_bb), which is inv(R)'s own diagonal block, on it.
-            frag[e] = (c < b) ? -real_form(Rs[i * LD + j], p, o) : real_form(Xs[i * LD + j], p, o);
-        }
-    }
+    solve_plan(Rs, Xs, k, plan, frag);
 }
 
 // Plain substitution, a thread per row (the reference's ztrsm arithmetic),

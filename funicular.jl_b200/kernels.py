@@ -299,24 +299,47 @@ def laplace7_apply(backend, dst: DeviceMatrix, src: DeviceMatrix, grid, shift) -
     return dst
 
 
-def cholqr2_batched_workspace_bytes(shapes) -> int:
-    """Device scratch for a batch of cholqr2! instances of the given (N, k)."""
+BATCH_SCHEDULES = ("auto", "persistent", "lanes")
+
+
+def batch_schedule(shapes, form: str = "fp64", schedule: str = "auto") -> str:
+    """The schedule a batch of (N, k) runs on: "persistent" (one persistent
+    kernel launch for the whole batch; FP64 form, every k <= 64) or "lanes"
+    (each instance's chain on one of eight forked streams, any k, either
+    form). "auto" takes the persistent kernel wherever it applies."""
+    if schedule not in BATCH_SCHEDULES:
+        raise ArgumentError(f"a batch schedule is one of {BATCH_SCHEDULES}, got {schedule!r}")
+    fits = form == "fp64" and all(int(k) <= 64 for _, k in shapes)
+    if schedule == "persistent" and not fits:
+        raise ArgumentError("the persistent batch kernel runs the FP64 form with every k <= 64")
+    if schedule == "auto":
+        return "persistent" if fits else "lanes"
+    return schedule
+
+
+def cholqr2_batched_workspace_bytes(shapes, form: str = "fp64", schedule: str = "auto") -> int:
+    """Device scratch for a batch of cholqr2! instances of the given (N, k)
+    on the schedule `batch_schedule` picks."""
     n = len(shapes)
     Ns = (ctypes.c_int64 * max(n, 1))(*[int(s[0]) for s in shapes])
     ks = (ctypes.c_int * max(n, 1))(*[int(s[1]) for s in shapes])
     need = ctypes.c_size_t(0)
-    call("fb_zcholqr2_batched_workspace_size", ctypes.cast(Ns, ctypes.c_void_p), ctypes.cast(ks, ctypes.c_void_p),
-         n, ctypes.byref(need))
+    entry = ("fb_zcholqr2_batched_persistent_workspace_size"
+             if batch_schedule(shapes, form, schedule) == "persistent" else "fb_zcholqr2_batched_workspace_size")
+    call(entry, ctypes.cast(Ns, ctypes.c_void_p), ctypes.cast(ks, ctypes.c_void_p), n, ctypes.byref(need))
     return need.value
 
 
-def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, workspace=None):
+def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, workspace=None,
+                    schedule: str = "auto"):
     """cholqr2! of many independent device matrices Ys[i] (N_i x k_i), R_i into
-    Rs[i], enqueued one after another on the current queue. With wait=True it
+    Rs[i], enqueued on the current queue as one persistent kernel launch or on
+    eight stream lanes (`schedule`, see batch_schedule). With wait=True it
     returns the list of passes and raises NotPositiveDefinite if an instance's
     Gram stayed indefinite. `workspace` = (pointer, bytes) of caller-owned
     scratch, which a captured graph needs (the backend's shared scratch may
-    move); by default the backend's is used."""
+    move), sized by cholqr2_batched_workspace_bytes with the same form and
+    schedule; by default the backend's is used."""
     if form not in ("fp64", "tc"):
         raise ArgumentError(f"cholqr2! form is 'fp64' or 'tc', got {form!r}")
     if len(Ys) != len(Rs):
@@ -328,6 +351,8 @@ def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, work
             raise DimensionMismatch(f"cholqr2! of an {Y.shape} matrix writes a {Y.cols}x{Y.cols} R, got {R.shape}")
     if n == 0:
         return []
+    shapes = [Y.shape for Y in Ys]
+    schedule = batch_schedule(shapes, form, schedule)
     arr = lambda ctype, vals: (ctype * n)(*vals)
     Yp = arr(ctypes.c_void_p, [Y.ptr for Y in Ys])
     ldy = arr(ctypes.c_int64, [Y.ld for Y in Ys])
@@ -338,13 +363,17 @@ def cholqr2_batched(backend, Ys, Rs, form: str = "fp64", wait: bool = True, work
     cast = lambda a: ctypes.cast(a, ctypes.c_void_p)
     own = workspace is None
     if own:
-        ws, ws_bytes = backend.workspace(cholqr2_batched_workspace_bytes([Y.shape for Y in Ys]))
+        ws, ws_bytes = backend.workspace(cholqr2_batched_workspace_bytes(shapes, form, schedule))
     else:
         ws, ws_bytes = workspace
     lib = _lib.load()
     try:
-        status = lib.fb_zcholqr2_batched(cast(Yp), cast(ldy), cast(Ns), cast(ks), cast(Rp), cast(ldr), n,
-                                         1 if form == "tc" else 0, _vp(ws), ws_bytes, backend.queue_handle())
+        if schedule == "persistent":
+            status = lib.fb_zcholqr2_batched_persistent(cast(Yp), cast(ldy), cast(Ns), cast(ks), cast(Rp),
+                                                        cast(ldr), n, _vp(ws), ws_bytes, backend.queue_handle())
+        else:
+            status = lib.fb_zcholqr2_batched(cast(Yp), cast(ldy), cast(Ns), cast(ks), cast(Rp), cast(ldr), n,
+                                             1 if form == "tc" else 0, _vp(ws), ws_bytes, backend.queue_handle())
     finally:
         if own:
             backend.workspace_release()

@@ -331,6 +331,24 @@ int fb_zcholqr2_batched(fb_z128* const* Y, const int64_t* ldy, const int64_t* N,
                         void* workspace, size_t workspace_bytes, fb_queue_t queue);
 int fb_zcholqr2_batched_query(const void* workspace, int count, int* info, int* passes);
 
+/* The same batch (the same arguments, status blocks and query) as ONE
+ * persistent kernel launch: a grid of one CTA per SM takes jobs from a ticket
+ * counter (the Gram chunks, factors and solve chunks of every pass of every
+ * instance), with device-side arrival counters and ready flags between them,
+ * so a batch is a memset and one launch (one more launch per 384 instances)
+ * and captures into a graph of those nodes. FP64 form, every k[i] <= 64
+ * (FB_ENOTSUP otherwise: fb_zcholqr2_batched takes any k). Each instance's
+ * bits depend only on its own (N, k), not on the rest of the batch, but its
+ * Gram chunking differs from fb_zcholqr2's, so they are not those of a single
+ * call. A device-side wait that gives up (2 s; it cannot happen unless the
+ * kernel is broken) stops the kernel and makes the query return FB_ECUDA.
+ * workspace: fb_zcholqr2_batched_persistent_workspace_size bytes, 256-byte
+ * aligned; read by fb_zcholqr2_batched_query after the queue drained. */
+int fb_zcholqr2_batched_persistent_workspace_size(const int64_t* N, const int* k, int count, size_t* bytes);
+int fb_zcholqr2_batched_persistent(fb_z128* const* Y, const int64_t* ldy, const int64_t* N, const int* k,
+                                   fb_z128* const* R, const int64_t* ldr, int count,
+                                   void* workspace, size_t workspace_bytes, fb_queue_t queue);
+
 /* ---- differentiation: the adjoints behind the rrules ------------------
  * The reference has no rrule (Project.toml:6-9 has no ChainRulesCore); these
  * are the kernels a ChainRulesCore.rrule for cholqr2! (src/panelblas.jl:130)

@@ -170,6 +170,17 @@ def test_newer_entry_points_check_arguments_without_a_gpu(fb):
     assert lib.fb_zcholqr2_batched_workspace_size(ctypes.cast(Ns, ctypes.c_void_p), ctypes.cast(ks, ctypes.c_void_p),
                                                    2, ctypes.byref(n)) == E.FB_EINVAL
     assert "instance 1" in E.last_error()
+    # The persistent batch: the same argument checks, and k past 64 refused.
+    assert lib.fb_zcholqr2_batched_persistent(None, None, None, None, None, None, 0, None, 0, None) == E.FB_OK
+    assert lib.fb_zcholqr2_batched_persistent(None, None, None, None, None, None, 2, None, 0, None) == E.FB_EINVAL
+    cast = lambda x: ctypes.cast(x, ctypes.c_void_p)
+    assert lib.fb_zcholqr2_batched_persistent_workspace_size(cast(Ns), cast(ks), 2, ctypes.byref(n)) == E.FB_EINVAL
+    Ns2 = (ctypes.c_int64 * 2)(100, 5000)
+    ks2 = (ctypes.c_int * 2)(64, 65)
+    assert lib.fb_zcholqr2_batched_persistent_workspace_size(cast(Ns2), cast(ks2), 2, ctypes.byref(n)) == E.FB_ENOTSUP
+    assert "instance 1" in E.last_error()
+    assert lib.fb_zcholqr2_batched_persistent_workspace_size(cast(Ns2), cast(ks2), 1, ctypes.byref(n)) == E.FB_OK
+    assert n.value > 0
     # The tuning table.
     assert lib.fb_tune_set_batch_lanes(0) == E.FB_EINVAL
     assert lib.fb_tune_set_batch_lanes(17) == E.FB_EINVAL

@@ -20,10 +20,10 @@
 // gives up after 2 s, marks the instance's status and stops the kernel.
 //
 // Gram job: a copy warp streams the chunk through shared memory in stages of
-// 32 rows with bulk copies (cp.async.bulk, one per column and stage, no
-// tensor map, so an instance needs no host-encoded descriptor), into a ring
-// of as many stages as 135 KB holds (4 at k = 64, 16 at k <= 16) guarded by
-// mbarriers. Twelve warps multiply on the FP64 tensor cores (mma m8n8k4 on
+// about 33 KB (32 rows at k = 64 up to 256 rows at k <= 8) with bulk copies
+// (cp.async.bulk, one per column and stage, no tensor map, so an instance
+// needs no host-encoded descriptor), into a ring of four to six stages
+// guarded by mbarriers. Twelve warps multiply on the FP64 tensor cores (mma m8n8k4 on
 // the real form of the complex product, as the chain's Gram kernel): the
 // upper triangle of 8 x 8 blocks is split into sets of block rows
 // {g, nb-1-g}, which carry equal MMA counts, each set owned by 12, 6, 4 or 3
@@ -35,7 +35,10 @@
 //
 // Solve jobs: the product by inv(R), the blocked solve or substitution, as
 // the plan says (the chain's paths, restated for a chunk of rows and the
-// CTA's sixteen warps). Data another CTA wrote during the launch is read
+// CTA's sixteen warps). Up to k = 32 the product by inv(R) reads its rows
+// through the same ring (15 warps multiply), which keeps 135 KB in flight
+// where one warp's own loads would not; wider panels load straight into
+// registers. Data another CTA wrote during the launch is read
 // through L2 (ld.global.cg), never from a possibly stale L1 line.
 #include <algorithm>
 #include <memory>
@@ -50,18 +53,23 @@ constexpr int PB_WARPS = 16;                         // warps of a CTA: four on 
 constexpr int PB_THREADS = PB_WARPS * 32;
 constexpr int PB_GRAM_WARPS = 12;                    // multiply in a Gram job; warp 12 issues its copies
 constexpr int PB_COPY_WARP = PB_GRAM_WARPS;
-constexpr int PB_SR = 32;                            // rows per Gram stage
-constexpr int PB_COL = PB_SR * 16 + 16;              // bytes per column in a stage: 32 rows, 16 of padding
-constexpr int PB_RING = 4 * 64 * PB_COL;             // ring bytes: four stages at k = 64
+constexpr int PB_SR_MAX = 256;                       // rows per Gram stage at k <= 8; chunks are multiples
+constexpr int PB_RING = 4 * 64 * (32 * 16 + 16);     // ring bytes: four stages of 32 rows at k = 64
 constexpr int PB_MAX_STAGES = 16;
 constexpr int PB_MAX_CHUNKS = 64;
 constexpr int PB_MAX_INST = 384;                     // instances per launch (kernel parameter space)
 constexpr int PB_PHASES = 6;
 constexpr int64_t PB_CHUNK_BYTES = 4 << 20;          // a chunk holds at least this much of Y
+constexpr int PB_STAGED_SOLVE_KMAX = 32;             // the product by inv(R) reads its rows through the ring up to here
 constexpr int PB_REGION = TR_KMAX * TR_PREP_LD * 16; // one k x k matrix of the factor step, padded
-constexpr int PB_SMEM = PB_RING;                     // >= 2 regions, >= solve fragments + transpose buffers
-static_assert(2 * PB_REGION <= PB_SMEM, "factor regions exceed the ring");
-static_assert(TR_FRAG_DOUBLES * 8 + PB_WARPS * TR_BUF * 16 <= PB_SMEM, "solve buffers exceed the ring");
+// Dynamic shared memory: the solve's B fragments, then the ring (which the
+// blocked solve's transpose buffers use when no copies run). The factor step
+// overlays both with its two k x k regions. Gram jobs leave the fragments in
+// place, so a CTA reuses them across its jobs until it runs a factor step.
+constexpr int PB_RING_OFF = TR_FRAG_DOUBLES * 8;
+constexpr int PB_SMEM = PB_RING_OFF + PB_RING;
+static_assert(2 * PB_REGION <= PB_SMEM, "factor regions exceed shared memory");
+static_assert(PB_WARPS * TR_BUF * 16 <= PB_RING, "transpose buffers exceed the ring");
 
 // Per instance, in the zeroed counter block (ints): arrivals of Gram chunks
 // by pass, factor-ready flags by pass, the last solved pass of each chunk.
@@ -90,6 +98,14 @@ static_assert(sizeof(PbArgs) <= 32764, "kernel parameters past the 32764-byte li
 __host__ __device__ inline size_t pb_align(size_t n) { return (n + 255) / 256 * 256; }
 __host__ __device__ inline int pb_kp(int k) { return (k + 7) / 8 * 8; }
 __host__ __device__ inline int pb_npairs(int k) { const int nb = pb_kp(k) / 8; return nb * (nb + 1) / 2; }
+
+// Rows of a Gram stage at nb 8-column blocks: about 33 KB of Y a stage at any
+// width (32 rows at k = 64, 256 at k <= 8), so narrow panels pay the ring's
+// barrier handshakes per as many bytes as wide ones. A column of a stage
+// takes its rows plus 16 bytes of padding, which puts the eight columns a
+// quarter warp reads in eight different bank groups.
+__host__ __device__ constexpr int pb_stage_rows(int nb) { return 32 * (8 / nb); }
+__host__ __device__ constexpr int pb_col_bytes(int nb) { return pb_stage_rows(nb) * 16 + 16; }
 
 // An instance's scratch: solve plan, B fragments, U, Ra (R1), Rb (R2 R1), and
 // the chunks' partial Gram matrices (8 x 8 blocks of the upper triangle,
@@ -148,9 +164,16 @@ __device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.pr
 // Named barrier over a Gram job's multiplying warps.
 __device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" ::"n"(PB_GRAM_WARPS * 32) : "memory"); }
 
-// Marks a wait that gave up: the instance's status says so and the kernel stops.
-__device__ void pb_timeout(const PbArgs& a, ChainStatus* st) {
-    atomicExch(&st->timeout, 1);
+// Where a wait gave up, as the status records it.
+enum PbWaitSite : int {
+    WAIT_GRAM_STAGE = 1, WAIT_GRAM_SLOT = 2, WAIT_SOLVE_STAGE = 3, WAIT_SOLVE_SLOT = 4,
+    WAIT_READY = 5, WAIT_SOLVED = 6,
+};
+
+// Marks a wait that gave up: the instance's status says where, and the
+// kernel stops taking jobs.
+__device__ void pb_timeout(const PbArgs& a, ChainStatus* st, int site) {
+    atomicCAS(&st->timeout, 0, site);
     atomicExch(a.ticket + 1, 1u);
 }
 
@@ -179,7 +202,7 @@ template <int NB, int G0>
 __device__ __forceinline__ void gram_kstep(const unsigned char* p, int odelta, unsigned long long flip,
                                            double (&acc)[GramSet<NB, G0>::NACC]) {
     using S = GramSet<NB, G0>;
-    constexpr int BLK = 8 * PB_COL;   // bytes from one 8-column block to the next
+    constexpr int BLK = 8 * pb_col_bytes(NB);   // bytes from one 8-column block to the next
     double own[S::NO];
 #pragma unroll
     for (int b = 0; b < S::NO; ++b) own[b] = *reinterpret_cast<const double*>(p + (S::R0 + b) * BLK);
@@ -210,34 +233,38 @@ struct GramCtx {
     unsigned char* ring;
     uint64_t* full;
     uint64_t* empty;
-    int stage_bytes, nslots, kp;
+    int stage_bytes, nslots, kp, sr, col_bytes;   // sr: rows a stage
     int64_t row0, row1;
     z64* out;           // this chunk's partial: npairs blocks of 64 entries
     bool ok;            // every stage arrived
+    int bad_site;       // the wait that gave up, if one did
 };
 
 // Waits for each stage of the chunk in turn, lets `work` multiply it, and
-// hands the slot back. The k-steps of the chunk (16 a stage) are dealt to the
+// hands the slot back. The k-steps of the chunk (SR / 2 a stage) are dealt to the
 // WPG warps of a set in turn, h, h + WPG, ..., across stage boundaries; work
 // gets the stage and its first k-step for this warp. A stage whose wait gave
 // up is skipped (ok = false), but the loop still runs to the end so every
 // multiplying warp passes the same named barriers. A short last stage with an
 // odd row count gets a zero row after its last row, so the k-step across it
 // adds nothing.
-template <int WPG, class Work>
+template <int WPG, int SR, class Work>
 __device__ __forceinline__ void gram_stages(GramCtx& c, uint32_t& full_par, int h, Work work) {
     const int lane = threadIdx.x & 31, ctid = threadIdx.x;
-    const int64_t nst = (c.row1 - c.row0 + PB_SR - 1) / PB_SR;
+    const int64_t nst = (c.row1 - c.row0 + SR - 1) / SR;
     int slot = 0, q0 = h;
     for (int64_t s = 0; s < nst; ++s) {
-        const bool got = mbar_wait(&c.full[slot], (full_par >> slot) & 1u);
+        const bool got = c.ok && mbar_wait(&c.full[slot], (full_par >> slot) & 1u);
         full_par ^= 1u << slot;
-        if (!got) c.ok = false;
-        const int valid = (int)min((int64_t)PB_SR, c.row1 - (c.row0 + s * PB_SR));
+        if (!got && c.ok) {
+            c.ok = false;
+            c.bad_site = WAIT_GRAM_STAGE;
+        }
+        const int valid = (int)min((int64_t)SR, c.row1 - (c.row0 + s * SR));
         unsigned char* base = c.ring + (size_t)slot * c.stage_bytes;
         if (valid & 1) {
             if (ctid < c.kp) {
-                *reinterpret_cast<z64*>(base + ctid * PB_COL + valid * 16) = zmake(0.0, 0.0);
+                *reinterpret_cast<z64*>(base + ctid * c.col_bytes + valid * 16) = zmake(0.0, 0.0);
                 fence_proxy_async_all();
             }
             compute_sync();
@@ -246,7 +273,7 @@ __device__ __forceinline__ void gram_stages(GramCtx& c, uint32_t& full_par, int 
         __syncwarp();
         if (lane == 0) mbar_arrive(&c.empty[slot]);
         if (++slot == c.nslots) slot = 0;
-        q0 = (q0 + 16 * WPG - PB_SR / 2) % WPG;
+        q0 = (q0 + SR / 2 * WPG - SR / 2) % WPG;
     }
 }
 
@@ -258,13 +285,14 @@ __device__ void gram_warp(GramCtx& c, uint32_t& full_par) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int h = warp % WPG;
     const int col8 = lane >> 2, t = (lane >> 1) & 1, part = lane & 1;
-    const int lane_off = col8 * PB_COL + t * 16 + part * 8;
+    constexpr int SR = pb_stage_rows(NB);
+    const int lane_off = col8 * pb_col_bytes(NB) + t * 16 + part * 8;
     const int odelta = part ? -8 : 8;
     const unsigned long long flip = part ? 0ull : 0x8000000000000000ull;
     double acc[S::NACC];
 #pragma unroll
     for (int i = 0; i < S::NACC; ++i) acc[i] = 0.0;
-    gram_stages<WPG>(c, full_par, h, [&](const unsigned char* base, int q0, int nq) {
+    gram_stages<WPG, SR>(c, full_par, h, [&](const unsigned char* base, int q0, int nq) {
         const unsigned char* p = base + lane_off;
 #pragma unroll 2
         for (int q = q0; q < nq; q += WPG) gram_kstep<NB, G0>(p + q * 32, odelta, flip, acc);
@@ -328,13 +356,14 @@ __device__ void gram_compute(GramCtx& c, uint32_t& full_par) {
 // the bytes on the slot's full barrier and copies each column's rows with one
 // bulk copy per lane and column. ok = false if a wait gave up (no more copies
 // are then issued; the multiplying warps' own waits give up too).
-__device__ void gram_produce(const z64* Y, int64_t ldy, int k, GramCtx& c, uint32_t& empty_par, uint32_t& used) {
+__device__ void gram_produce(const z64* Y, int64_t ldy, int k, GramCtx& c, uint32_t& empty_par, uint32_t& used,
+                             int copy_site) {
     const int lane = threadIdx.x & 31;
-    const int64_t nst = (c.row1 - c.row0 + PB_SR - 1) / PB_SR;
+    const int64_t nst = (c.row1 - c.row0 + c.sr - 1) / c.sr;
     int slot = 0;
     for (int64_t s = 0; s < nst; ++s) {
-        const int64_t r = c.row0 + s * PB_SR;
-        const int valid = (int)min((int64_t)PB_SR, c.row1 - r);
+        const int64_t r = c.row0 + s * c.sr;
+        const int valid = (int)min((int64_t)c.sr, c.row1 - r);
         const bool reuse = (used >> slot) & 1u;
         int good = 1;
         if (lane == 0 && c.ok) {
@@ -345,12 +374,13 @@ __device__ void gram_produce(const z64* Y, int64_t ldy, int k, GramCtx& c, uint3
         if (reuse) empty_par ^= 1u << slot;
         used |= 1u << slot;
         if (!good) {
+            if (c.ok) c.bad_site = copy_site;
             c.ok = false;
         } else {
             __syncwarp();
             unsigned char* dst = c.ring + (size_t)slot * c.stage_bytes;
             for (int col = lane; col < k; col += 32)
-                bulk_load(dst + col * PB_COL, Y + r + (int64_t)col * ldy, (uint32_t)valid * 16, &c.full[slot]);
+                bulk_load(dst + col * c.col_bytes, Y + r + (int64_t)col * ldy, (uint32_t)valid * 16, &c.full[slot]);
         }
         if (++slot == c.nslots) slot = 0;
     }
@@ -480,13 +510,90 @@ __device__ void factor_step(const PbInst& I, int pass, unsigned char* smem, doub
 
 // ---- solve jobs ------------------------------------------------------------------
 
-// Y inv(R) for the 8-row units [u0, u1), a unit a warp at a time. As the
-// chain's product by the inverse: a warp loads its 8 rows once in the MMA A
-// layout, n-tile t needs k-steps 0..2t+1 only, and the fragment loads of
-// tile t wait for the result of tile t - 2.
+// Y inv(R) for the rows of a chunk that the copy warp streams through the
+// ring (stages of c.sr rows, c.sr / 8 units of 8 rows a stage), so up to
+// 135 KB of Y is in flight per SM whatever k is. The fifteen other warps
+// pass every stage in order, as a Gram job's warps do: wait for it, load the
+// rows of their own units (unit u belongs to warp u mod 15) in the MMA A
+// layout, hand the slot back (fifteen hand-backs free it), then multiply as
+// the chain's product by the inverse does: n-tile t needs k-steps 0..2t+1
+// only, and the fragment loads of tile t wait for the result of tile t - 2.
+// Since no slot is refilled before every warp has passed it, a warp always
+// waits on the phase right after the one it saw last.
 template <int NT>
-__device__ void pb_solve_inverse(z64* Y, int64_t ldy, int64_t rows, int k, int64_t u0, int64_t u1,
+__device__ void pb_solve_inverse(GramCtx& c, uint32_t& full_par, z64* Y, int64_t ldy, int64_t rows, int k,
                                  const double* frag, int zero) {
+    constexpr int NS = 2 * NT;
+    constexpr int NSW = PB_WARPS - 1;   // solving warps: all but the copy warp
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sw = warp < PB_COPY_WARP ? warp : warp - 1;
+    const int cq = lane & 3, acol = cq >> 1, apart = lane & 1, rr = lane >> 2;
+    const int ups = c.sr / 8;
+    const int64_t nunits = (c.row1 - c.row0 + 7) / 8;
+    const int64_t nst = (c.row1 - c.row0 + c.sr - 1) / c.sr;
+    int slot = 0;
+    for (int64_t st = 0; st < nst; ++st) {
+        const bool got = c.ok && mbar_wait(&c.full[slot], (full_par >> slot) & 1u);
+        full_par ^= 1u << slot;
+        if (!got && c.ok) {
+            c.ok = false;
+            c.bad_site = WAIT_SOLVE_STAGE;
+        }
+        const unsigned char* stage = c.ring + (size_t)slot * c.stage_bytes;
+        const int64_t first = st * ups, end = min(nunits, first + ups);
+        // This warp's first unit in the stage: the least u >= first with u = sw (mod 15).
+        int64_t u = first + ((sw - first % NSW) % NSW + NSW) % NSW;
+        if (u >= end) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&c.empty[slot]);
+        }
+        for (; u < end; u += NSW) {
+            const unsigned char* base = stage + ((int)(u - first) * 8 + rr) * 16 + apart * 8;
+            double a[NS];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int col = 2 * s + acol;
+                a[s] = (got && col < k) ? *reinterpret_cast<const double*>(base + col * c.col_bytes) : 0.0;
+            }
+            if (u + NSW >= end) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&c.empty[slot]);
+            }
+            const int64_t row = c.row0 + u * 8 + rr;
+            const bool live = row < rows;
+            z64* yrow = Y + (live ? row : 0);
+            double chain = 0.0, done1 = 0.0, done2 = 0.0;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                double acc[2][2] = {};
+                const double* fp = frag + 32 * t * (t + 1) + lane;
+                chain = done2;
+#pragma unroll
+                for (int s = 0; s <= 2 * t + 1; ++s) {
+                    if ((s & 7) == 0) fp = hold(fp, chain, zero);
+                    const double bv = fp[s * 32];
+                    if ((s & 7) == 0) chain = bv;
+                    dmma_884(acc[s & 1][0], acc[s & 1][1], a[s], bv);
+                }
+                const int col = 4 * t + cq;
+                const z64 x = zmake(acc[0][0] + acc[1][0], acc[0][1] + acc[1][1]);
+                if (live && col < k) __stcg(yrow + (int64_t)col * ldy, x);
+                done2 = done1;
+                done1 = x.x;
+            }
+        }
+        if (++slot == c.nslots) slot = 0;
+    }
+}
+
+// Y inv(R) with each warp loading its own units' rows straight into
+// registers (a unit of 8 rows at a time, all sixteen warps): for wide panels
+// (k > 32), where a unit's 4k loads already keep enough bytes in flight and
+// its products are long, so the ring's stage-by-stage hand-backs only hold
+// the warps back. Per unit as pb_solve_inverse.
+template <int NT>
+__device__ void pb_solve_inverse_direct(z64* Y, int64_t ldy, int64_t rows, int k, int64_t u0, int64_t u1,
+                                        const double* frag, int zero) {
     constexpr int NS = 2 * NT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cq = lane & 3, acol = cq >> 1, apart = lane & 1, rr = lane >> 2;
@@ -494,8 +601,8 @@ __device__ void pb_solve_inverse(z64* Y, int64_t ldy, int64_t rows, int k, int64
         const int64_t row = u * 8 + rr;
         const bool live = row < rows;
         z64* yrow = Y + (live ? row : 0);
-        double a[NS];
         const double* y = reinterpret_cast<const double*>(yrow) + apart;
+        double a[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int col = 2 * s + acol;
@@ -641,16 +748,43 @@ __device__ void pb_solve_substitute(z64* Y, int64_t ldy, int64_t row0, int64_t r
 
 // ---- jobs and the kernel -------------------------------------------------------------
 
+// The ring's barriers as one kind of job uses them: Gram jobs and solve jobs
+// have a set each (their empty barriers count 12 and 15 hand-backs a stage),
+// initialized once. Every waiting warp passes every stage of every job of its
+// kind, so the per-slot phase parities below, kept across jobs, stay the same
+// in every thread of the CTA whatever the slot count of a job is.
 struct PbRing {
     uint64_t* full;
     uint64_t* empty;
     uint32_t full_par, empty_par, used;   // per slot: phase parities, and whether it was ever filled
 };
 
+// The ring of a job over the rows of `chunk` (stage height and slot count by
+// the instance's width).
+__device__ GramCtx ring_ctx(const PbInst& I, int chunk, unsigned char* smem, const PbRing& ring) {
+    const int kp = pb_kp(I.k);
+    GramCtx c;
+    c.ring = smem + PB_RING_OFF;
+    c.full = ring.full;
+    c.empty = ring.empty;
+    c.sr = pb_stage_rows(kp / 8);
+    c.col_bytes = pb_col_bytes(kp / 8);
+    c.stage_bytes = kp * c.col_bytes;
+    c.nslots = min(PB_MAX_STAGES, PB_RING / c.stage_bytes);
+    c.kp = kp;
+    c.row0 = (int64_t)chunk * I.chunk_rows;
+    c.row1 = min(I.N, c.row0 + I.chunk_rows);
+    c.out = nullptr;
+    c.ok = true;
+    c.bad_site = 0;
+    return c;
+}
+
 // The Gram chunk `chunk` of pass `pass`: waits (pass >= 2) for the chunk's
 // solve of the previous pass, multiplies unless the instance stopped, adds
 // the arrival, and runs the factor step if it was the last chunk to arrive.
-__device__ void gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, unsigned char* smem, PbRing& ring,
+// Returns whether it ran the factor step (which overwrites the fragments).
+__device__ bool gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, unsigned char* smem, PbRing& ring,
                          double* red) {
     __shared__ int s_skip, s_bad, s_last;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -659,7 +793,7 @@ __device__ void gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
         int skip = 0;
         if (pass >= 2) {
             if (!wait_flag(I.counters + PB_SOLVED + chunk, pass - 1)) {
-                pb_timeout(a, st);
+                pb_timeout(a, st, WAIT_SOLVED);
                 skip = 1;
             } else {
                 skip = __ldcg(&st->failed) != 0 || __ldcg(&st->timeout) != 0;
@@ -671,24 +805,16 @@ __device__ void gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
     }
     __syncthreads();
     if (!s_skip) {
-        const int k = I.k, kp = pb_kp(k);
-        GramCtx c;
-        c.ring = smem;
-        c.full = ring.full;
-        c.empty = ring.empty;
-        c.stage_bytes = kp * PB_COL;
-        c.nslots = min(PB_MAX_STAGES, PB_RING / c.stage_bytes);
-        c.kp = kp;
-        c.row0 = (int64_t)chunk * I.chunk_rows;
-        c.row1 = min(I.N, c.row0 + I.chunk_rows);
+        const int k = I.k;
+        GramCtx c = ring_ctx(I, chunk, smem, ring);
         c.out = reinterpret_cast<z64*>(I.scratch + pb_layout(k, I.nchunks).partial) + (size_t)chunk * pb_npairs(k) * 64;
-        c.ok = true;
         // Padding columns past k read as zero: no copy writes them.
-        if (k < kp) {
-            for (int e = tid; e < c.nslots * (kp - k) * PB_SR; e += blockDim.x) {
-                const int slot = e / ((kp - k) * PB_SR), rem = e - slot * (kp - k) * PB_SR;
-                const int col = k + rem / PB_SR, row = rem % PB_SR;
-                *reinterpret_cast<z64*>(smem + (size_t)slot * c.stage_bytes + col * PB_COL + row * 16) = zmake(0.0, 0.0);
+        if (k < c.kp) {
+            for (int e = tid; e < c.nslots * (c.kp - k) * c.sr; e += blockDim.x) {
+                const int slot = e / ((c.kp - k) * c.sr), rem = e - slot * (c.kp - k) * c.sr;
+                const int col = k + rem / c.sr, row = rem % c.sr;
+                *reinterpret_cast<z64*>(c.ring + (size_t)slot * c.stage_bytes + col * c.col_bytes + row * 16) =
+                    zmake(0.0, 0.0);
             }
         }
         // Whatever this CTA last wrote into the ring through generic stores is
@@ -696,29 +822,29 @@ __device__ void gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
         fence_proxy_async_all();
         __syncthreads();
         if (warp == PB_COPY_WARP) {
-            gram_produce(I.Y, I.ldy, k, c, ring.empty_par, ring.used);
+            gram_produce(I.Y, I.ldy, k, c, ring.empty_par, ring.used, WAIT_GRAM_SLOT);
         } else if (warp < PB_GRAM_WARPS) {
-            switch (kp / 8) {
+            switch (c.kp / 8) {
 #define FB_PB_GRAM(n) case n: gram_compute<n>(c, ring.full_par); break;
                 FB_PB_GRAM(1) FB_PB_GRAM(2) FB_PB_GRAM(3) FB_PB_GRAM(4)
                 FB_PB_GRAM(5) FB_PB_GRAM(6) FB_PB_GRAM(7) FB_PB_GRAM(8)
 #undef FB_PB_GRAM
             }
         }
-        if (!c.ok) s_bad = 1;
+        if (!c.ok) s_bad = c.bad_site;
     }
     __syncthreads();
     if (tid == 0) {
-        if (s_bad) pb_timeout(a, st);
+        if (s_bad) pb_timeout(a, st, s_bad);
         __threadfence();
         const int before = atomicAdd(I.counters + PB_ARRIVE + pass, 1);
         s_last = before == I.nchunks - 1;
     }
     __syncthreads();
-    if (s_last) {
-        __threadfence();
-        factor_step(I, pass, smem, red);
-    }
+    if (!s_last) return false;
+    __threadfence();
+    factor_step(I, pass, smem, red);
+    return true;
 }
 
 // The solve chunk `chunk` of pass `pass`: waits for the pass's factor, solves
@@ -726,29 +852,30 @@ __device__ void gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
 // marks the chunk solved for this pass. `cached` names the fragments already
 // in shared memory (instance slot * 4 + pass, -1 for none).
 __device__ void solve_job(const PbArgs& a, const PbInst& I, int slot, int pass, int chunk, unsigned char* smem,
-                          int& cached) {
-    __shared__ int s_skip, s_path;
-    const int tid = threadIdx.x;
+                          PbRing& ring, int& cached) {
+    // ring: the solve jobs' barrier set.
+    __shared__ int s_skip, s_path, s_bad;
+    const int tid = threadIdx.x, warp = tid >> 5;
     ChainStatus* st = I.st;
     const int k = I.k;
     const PbLayout L = pb_layout(k, I.nchunks);
     if (tid == 0) {
         int skip = 0;
         if (!wait_flag(I.counters + PB_READY + pass, 1)) {
-            pb_timeout(a, st);
+            pb_timeout(a, st, WAIT_READY);
             skip = 1;
         } else {
             skip = __ldcg(&st->failed) != 0 || __ldcg(&st->timeout) != 0;
             if (pass == 3) skip = skip || !(__ldcg(&st->shifted[1]) | __ldcg(&st->shifted[2]));
         }
         s_skip = skip;
+        s_bad = 0;
         s_path = skip ? PATH_SUBSTITUTE : __ldcg(&reinterpret_cast<const TrsmPlan*>(I.scratch + L.plan)->path);
     }
     __syncthreads();
     if (!s_skip) {
         const int path = s_path;
         double* frag = reinterpret_cast<double*>(smem);
-        z64* tbuf = reinterpret_cast<z64*>(smem + TR_FRAG_DOUBLES * 8);
         const int key = slot * 4 + pass;
         if (cached != key) {
             const int n = path == PATH_INVERSE ? inverse_frag_doubles(k)
@@ -756,34 +883,50 @@ __device__ void solve_job(const PbArgs& a, const PbInst& I, int slot, int pass, 
             const double2* src = reinterpret_cast<const double2*>(I.scratch + L.frag);
             for (int e = tid; e < n / 2; e += blockDim.x) reinterpret_cast<double2*>(frag)[e] = __ldcg(src + e);
             cached = key;
-            __syncthreads();
         }
-        const int64_t row0 = (int64_t)chunk * I.chunk_rows;
-        const int64_t row1 = min(I.N, row0 + I.chunk_rows);
-        const int64_t u0 = row0 / 8, u1 = (row1 + 7) / 8;
-        if (path == PATH_INVERSE) {
-            switch ((k + 3) / 4) {
-#define FB_PB_INV(n) case n: pb_solve_inverse<n>(I.Y, I.ldy, I.N, k, u0, u1, frag, a.zero); break;
-                FB_PB_INV(1) FB_PB_INV(2) FB_PB_INV(3) FB_PB_INV(4) FB_PB_INV(5) FB_PB_INV(6)
-                FB_PB_INV(7) FB_PB_INV(8) FB_PB_INV(9) FB_PB_INV(10) FB_PB_INV(11) FB_PB_INV(12)
-                FB_PB_INV(13) FB_PB_INV(14) FB_PB_INV(15) FB_PB_INV(16)
+        GramCtx c = ring_ctx(I, chunk, smem, ring);
+        if (path == PATH_INVERSE && k <= PB_STAGED_SOLVE_KMAX) {
+            fence_proxy_async_all();
+            __syncthreads();
+            if (warp == PB_COPY_WARP) {
+                gram_produce(I.Y, I.ldy, k, c, ring.empty_par, ring.used, WAIT_SOLVE_SLOT);
+            } else {
+                switch ((k + 3) / 4) {
+#define FB_PB_INV(n) case n: pb_solve_inverse<n>(c, ring.full_par, I.Y, I.ldy, I.N, k, frag, a.zero); break;
+                    FB_PB_INV(1) FB_PB_INV(2) FB_PB_INV(3) FB_PB_INV(4)
+                    FB_PB_INV(5) FB_PB_INV(6) FB_PB_INV(7) FB_PB_INV(8)
 #undef FB_PB_INV
+                }
             }
-        } else if (path == PATH_BLOCKED) {
-            switch (pb_kp(k) / 8) {
-#define FB_PB_BLK(n) case n: pb_solve_blocked<n>(I.Y, I.ldy, I.N, k, u0, u1, frag, tbuf); break;
-                FB_PB_BLK(1) FB_PB_BLK(2) FB_PB_BLK(3) FB_PB_BLK(4)
-                FB_PB_BLK(5) FB_PB_BLK(6) FB_PB_BLK(7) FB_PB_BLK(8)
-#undef FB_PB_BLK
-            }
+            if (!c.ok) s_bad = c.bad_site;
         } else {
-            pb_solve_substitute(I.Y, I.ldy, row0, row1, k, reinterpret_cast<const z64*>(I.scratch + L.U));
+            __syncthreads();
+            const int64_t u0 = c.row0 / 8, u1 = (c.row1 + 7) / 8;
+            if (path == PATH_INVERSE) {
+                switch ((k + 3) / 4) {
+#define FB_PB_INV(n) case n: pb_solve_inverse_direct<n>(I.Y, I.ldy, I.N, k, u0, u1, frag, a.zero); break;
+                    FB_PB_INV(9) FB_PB_INV(10) FB_PB_INV(11) FB_PB_INV(12)
+                    FB_PB_INV(13) FB_PB_INV(14) FB_PB_INV(15) FB_PB_INV(16)
+#undef FB_PB_INV
+                }
+            } else if (path == PATH_BLOCKED) {
+                z64* tbuf = reinterpret_cast<z64*>(smem + PB_RING_OFF);
+                switch (pb_kp(k) / 8) {
+#define FB_PB_BLK(n) case n: pb_solve_blocked<n>(I.Y, I.ldy, I.N, k, u0, u1, frag, tbuf); break;
+                    FB_PB_BLK(1) FB_PB_BLK(2) FB_PB_BLK(3) FB_PB_BLK(4)
+                    FB_PB_BLK(5) FB_PB_BLK(6) FB_PB_BLK(7) FB_PB_BLK(8)
+#undef FB_PB_BLK
+                }
+            } else {
+                pb_solve_substitute(I.Y, I.ldy, c.row0, c.row1, k, reinterpret_cast<const z64*>(I.scratch + L.U));
+            }
         }
         // The next pass's Gram reads these rows with bulk copies.
         fence_proxy_async_all();
     }
     __syncthreads();
     if (tid == 0) {
+        if (s_bad) pb_timeout(a, st, s_bad);
         __threadfence();
         st_release(I.counters + PB_SOLVED + chunk, pass);
     }
@@ -791,19 +934,23 @@ __device__ void solve_job(const PbArgs& a, const PbInst& I, int slot, int pass, 
 
 __global__ void __launch_bounds__(PB_THREADS, 1) batch_chain_kernel(const __grid_constant__ PbArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t full[PB_MAX_STAGES], empty[PB_MAX_STAGES];
+    __shared__ uint64_t gfull[PB_MAX_STAGES], gempty[PB_MAX_STAGES];
+    __shared__ uint64_t sfull[PB_MAX_STAGES], sempty[PB_MAX_STAGES];
     __shared__ double red[33];
     __shared__ int s_job;
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int b = 0; b < PB_MAX_STAGES; ++b) {
-            mbar_init(&full[b], 1);
-            mbar_init(&empty[b], PB_GRAM_WARPS);
+            mbar_init(&gfull[b], 1);
+            mbar_init(&gempty[b], PB_GRAM_WARPS);
+            mbar_init(&sfull[b], 1);
+            mbar_init(&sempty[b], PB_WARPS - 1);
         }
         mbar_fence_init();
     }
     __syncthreads();
-    PbRing ring{full, empty, 0u, 0u, 0u};
+    PbRing gring{gfull, gempty, 0u, 0u, 0u};
+    PbRing sring{sfull, sempty, 0u, 0u, 0u};
     int cached = -1;
     const int total = PB_PHASES * a.jobs;
     for (;;) {
@@ -825,10 +972,9 @@ __global__ void __launch_bounds__(PB_THREADS, 1) batch_chain_kernel(const __grid
         const PbInst& I = a.inst[lo];
         const int pass = phase / 2 + 1, chunk = j - I.first_job;
         if ((phase & 1) == 0) {
-            gram_job(a, I, pass, chunk, smem, ring, red);
-            cached = -1;
+            if (gram_job(a, I, pass, chunk, smem, gring, red)) cached = -1;
         } else {
-            solve_job(a, I, lo, pass, chunk, smem, cached);
+            solve_job(a, I, lo, pass, chunk, smem, sring, cached);
         }
         __syncthreads();
     }
@@ -841,13 +987,13 @@ using namespace fb;
 namespace {
 
 // Rows a chunk of an N x k instance holds: at least PB_CHUNK_BYTES of Y, at
-// most 64 chunks, a multiple of the stage height.
+// most 64 chunks, a multiple of every stage height.
 void pb_chunking(int64_t N, int k, int& chunk_rows, int& nchunks) {
     int64_t rows = PB_CHUNK_BYTES / (16 * (int64_t)k);
     const int64_t spread = (N + PB_MAX_CHUNKS - 1) / PB_MAX_CHUNKS;
     if (rows < spread) rows = spread;
-    rows = (rows + PB_SR - 1) / PB_SR * PB_SR;
-    const int64_t whole = (N + PB_SR - 1) / PB_SR * PB_SR;
+    rows = (rows + PB_SR_MAX - 1) / PB_SR_MAX * PB_SR_MAX;
+    const int64_t whole = (N + PB_SR_MAX - 1) / PB_SR_MAX * PB_SR_MAX;
     if (rows > whole) rows = whole;
     chunk_rows = (int)rows;
     nchunks = (int)((N + rows - 1) / rows);

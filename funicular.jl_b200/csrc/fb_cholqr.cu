@@ -331,8 +331,11 @@ int fb_zcholqr2_query(const void* workspace, int* info, int* passes, double* shi
     ChainStatus host{};
     FB_CUDA(cudaMemcpy(&host, workspace, sizeof host, cudaMemcpyDeviceToHost), "cudaMemcpy");
     if (host.timeout) {
-        set_error(FB_ECUDA, "cholqr2! batch: a device-side wait of the persistent kernel gave up after its 2 s "
-                  "limit, so the results are not valid");
+        static const char* const sites[] = {"?", "a Gram stage", "a Gram copy slot", "a solve stage",
+                                            "a solve copy slot", "a factor-ready flag", "a chunk-solved flag"};
+        const int site = host.timeout >= 1 && host.timeout <= 6 ? host.timeout : 0;
+        set_error(FB_ECUDA, "cholqr2! batch: a device-side wait of the persistent kernel (on %s) gave up after its "
+                  "2 s limit, so the results are not valid", sites[site]);
         return FB_ECUDA;
     }
     if (info) *info = host.failed;

@@ -84,7 +84,7 @@ __device__ __forceinline__ z64 zmul(z64 a, z64 b) {
 struct ChainStatus {
     int failed;        // 0, or the pass (1-based) whose Gram was not positive definite
     int shifted[4];    // shifted[p] = 1 when pass p factored G + sI
-    int timeout;       // 1 when a device-side wait of the batch kernel gave up
+    int timeout;       // where a device-side wait of the batch kernel gave up (0: none)
     int pad[2];
     double shift[4];   // the shift s of pass p, when one was taken
     double norm[4];    // ||G||_F of pass p

@@ -70,7 +70,8 @@ def parse_args():
     p.add_argument("--adjoint-N", type=int, default=1 << 22,
                    help="rows of the differentiation workload (0 skips it)")
     p.add_argument("--only", choices=("gram", "gram_tc", "trsm_blocked", "trsm_inverse", "ghost_fill", "laplace",
-                                      "cholqr2", "cholqr2_adjoint", "project_adjoint", "hband", "adjoint_step"),
+                                      "cholqr2", "cholqr2_adjoint", "project_adjoint", "hband", "adjoint_step",
+                                      "batch"),
                    default=None,
                    help="launch one kernel of the step on the workload, the timed launches inside an NVTX range "
                         "named 'only' (what a profiler capture selects), and print its time")
@@ -1249,6 +1250,8 @@ def run_only(args):
     backend = fb.B200Backend(0)
     if args.only == "laplace":
         return run_only_laplace(args, fb, backend, torch, device)
+    if args.only == "batch":
+        return run_only_batch(args, fb, backend, torch, device)
     if args.only in ("cholqr2_adjoint", "project_adjoint", "hband", "adjoint_step"):
         return run_only_adjoint(args, fb, backend, torch, device)
     Yt = build_workload(fb, backend, torch, device, N, k, seed=0xDEADBEEF)
@@ -1338,6 +1341,45 @@ def run_only_adjoint(args, fb, backend, torch, device):
     b.synchronize()
     print(json.dumps({"only": args.only, "N": N, "k": k, "kd": kd, "steps": args.steps,
                       "ms_per_launch": a.elapsed_time(b) / args.steps}), flush=True)
+    return 0
+
+
+def run_only_batch(args, fb, backend, torch, device):
+    """The persistent batch kernel on args.batch instances drawn as the bench's
+    batch section draws them (N log-uniform on [1e4, 2e6], k from {16, 32, 64},
+    the same seed): one launch per step."""
+    rng = np.random.default_rng(0xBA7C4)
+    Ns = np.exp(rng.uniform(np.log(1e4), np.log(2e6), args.batch)).astype(np.int64)
+    ks = rng.choice([16, 32, 64], args.batch)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(0xBA7C4)
+    tensors = [torch.randn((int(k), int(N)), dtype=torch.complex128, device=device, generator=gen)
+               for N, k in zip(Ns, ks)]
+    Ys = [wrap(fb, t, int(N), int(k)) for t, N, k in zip(tensors, Ns, ks)]
+    Rs = [backend.alloc_device(np.complex128, (int(k), int(k))) for k in ks]
+    shapes = [(int(N), int(k)) for N, k in zip(Ns, ks)]
+    nbytes = fb.kernels.cholqr2_batched_workspace_bytes(shapes, schedule="persistent")
+    buf = backend.alloc_device(np.complex128, (nbytes // 16 + 32, 1))
+    ws = ((buf.ptr + 255) // 256 * 256, nbytes)
+    torch.cuda.synchronize()
+    queue = backend.make_queue()
+    stream = torch.cuda.ExternalStream(queue.handle, device=device)
+    launch = lambda: fb.kernels.cholqr2_batched(backend, Ys, Rs, wait=False, workspace=ws, schedule="persistent")
+    for _ in range(args.warmup):
+        backend.submit(queue, launch)
+    backend.sync_queue(queue)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("only")
+    a.record(stream)
+    for _ in range(args.steps):
+        backend.submit(queue, launch)
+    b.record(stream)
+    torch.cuda.nvtx.range_pop()
+    b.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    print(json.dumps({"only": "batch", "instances": args.batch, "bytes_on_device": int(sum(16 * N * k for N, k in shapes)),
+                      "alg_bytes": float(sum(96.0 * N * k for N, k in shapes)), "ms_per_launch": ms}), flush=True)
     return 0
 
 

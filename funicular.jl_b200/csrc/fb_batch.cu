@@ -101,11 +101,16 @@ __host__ __device__ inline int pb_npairs(int k) { const int nb = pb_kp(k) / 8; r
 
 // Rows of a Gram stage at nb 8-column blocks: about 33 KB of Y a stage at any
 // width (32 rows at k = 64, 256 at k <= 8), so narrow panels pay the ring's
-// barrier handshakes per as many bytes as wide ones. A column of a stage
-// takes its rows plus 16 bytes of padding, which puts the eight columns a
-// quarter warp reads in eight different bank groups.
+// barrier handshakes per as many bytes as wide ones. A column of a Gram stage
+// takes its rows plus 16 bytes of padding: with a k-step's two rows 4 apart
+// (rows r and r + 4 of a group of 8), the half warp's eight columns and two
+// rows land in eight different 16-byte bank groups.
 __host__ __device__ constexpr int pb_stage_rows(int nb) { return 32 * (8 / nb); }
 __host__ __device__ constexpr int pb_col_bytes(int nb) { return pb_stage_rows(nb) * 16 + 16; }
+// Solve stages pad a column by 64 bytes instead: a quarter warp's A-fragment
+// load takes 4 rows of two adjacent columns, which this puts in the two
+// halves of the bank space.
+__host__ __device__ constexpr int pb_solve_col_bytes(int nb) { return pb_stage_rows(nb) * 16 + 64; }
 
 // An instance's scratch: solve plan, B fragments, U, Ra (R1), Rb (R2 R1), and
 // the chunks' partial Gram matrices (8 x 8 blocks of the upper triangle,
@@ -193,8 +198,8 @@ struct GramSet {
     static constexpr int NACC = B1 + (TWO ? 2 + 4 * OFF1 : 0);
 };
 
-// One k-step (two complex rows) of the set's blocks. p: this lane's own part
-// of column block 0 in the stage, at the k-step's rows; odelta: from there to
+// One k-step (two complex rows, 4 apart) of the set's blocks. p: this lane's
+// own part of column block 0 in the stage, at the k-step's rows; odelta: from there to
 // the lane's other part; flip: the sign bit that turns the other part into
 // the J W entry. Sums: a diagonal block S (2 doubles: D[li][lj], lj = 2 (lane
 // & 3) + 0/1), an off-diagonal block Re then Im (4 doubles).
@@ -245,9 +250,9 @@ struct GramCtx {
 // WPG warps of a set in turn, h, h + WPG, ..., across stage boundaries; work
 // gets the stage and its first k-step for this warp. A stage whose wait gave
 // up is skipped (ok = false), but the loop still runs to the end so every
-// multiplying warp passes the same named barriers. A short last stage with an
-// odd row count gets a zero row after its last row, so the k-step across it
-// adds nothing.
+// multiplying warp passes the same named barriers. A short last stage whose
+// row count is not a multiple of 8 gets zero rows up to the next multiple,
+// so the k-steps across them add nothing.
 template <int WPG, int SR, class Work>
 __device__ __forceinline__ void gram_stages(GramCtx& c, uint32_t& full_par, int h, Work work) {
     const int lane = threadIdx.x & 31, ctid = threadIdx.x;
@@ -262,14 +267,14 @@ __device__ __forceinline__ void gram_stages(GramCtx& c, uint32_t& full_par, int 
         }
         const int valid = (int)min((int64_t)SR, c.row1 - (c.row0 + s * SR));
         unsigned char* base = c.ring + (size_t)slot * c.stage_bytes;
-        if (valid & 1) {
-            if (ctid < c.kp) {
-                *reinterpret_cast<z64*>(base + ctid * c.col_bytes + valid * 16) = zmake(0.0, 0.0);
-                fence_proxy_async_all();
-            }
+        if (valid & 7) {
+            const int pad = 8 - (valid & 7);
+            for (int e = ctid; e < c.kp * pad; e += PB_GRAM_WARPS * 32)
+                *reinterpret_cast<z64*>(base + (e / pad) * c.col_bytes + (valid + e % pad) * 16) = zmake(0.0, 0.0);
+            fence_proxy_async_all();
             compute_sync();
         }
-        if (got) work(base, q0, (valid + 1) >> 1);
+        if (got) work(base, q0, (valid + 7) / 8 * 4);
         __syncwarp();
         if (lane == 0) mbar_arrive(&c.empty[slot]);
         if (++slot == c.nslots) slot = 0;
@@ -286,7 +291,7 @@ __device__ void gram_warp(GramCtx& c, uint32_t& full_par) {
     const int h = warp % WPG;
     const int col8 = lane >> 2, t = (lane >> 1) & 1, part = lane & 1;
     constexpr int SR = pb_stage_rows(NB);
-    const int lane_off = col8 * pb_col_bytes(NB) + t * 16 + part * 8;
+    const int lane_off = col8 * pb_col_bytes(NB) + t * 64 + part * 8;
     const int odelta = part ? -8 : 8;
     const unsigned long long flip = part ? 0ull : 0x8000000000000000ull;
     double acc[S::NACC];
@@ -295,7 +300,7 @@ __device__ void gram_warp(GramCtx& c, uint32_t& full_par) {
     gram_stages<WPG, SR>(c, full_par, h, [&](const unsigned char* base, int q0, int nq) {
         const unsigned char* p = base + lane_off;
 #pragma unroll 2
-        for (int q = q0; q < nq; q += WPG) gram_kstep<NB, G0>(p + q * 32, odelta, flip, acc);
+        for (int q = q0; q < nq; q += WPG) gram_kstep<NB, G0>(p + (q >> 2) * 128 + (q & 3) * 16, odelta, flip, acc);
     });
     // The ring is free once every multiplying warp is past its last stage.
     double* comb = reinterpret_cast<double*>(c.ring);
@@ -761,14 +766,14 @@ struct PbRing {
 
 // The ring of a job over the rows of `chunk` (stage height and slot count by
 // the instance's width).
-__device__ GramCtx ring_ctx(const PbInst& I, int chunk, unsigned char* smem, const PbRing& ring) {
+__device__ GramCtx ring_ctx(const PbInst& I, int chunk, unsigned char* smem, const PbRing& ring, bool solve) {
     const int kp = pb_kp(I.k);
     GramCtx c;
     c.ring = smem + PB_RING_OFF;
     c.full = ring.full;
     c.empty = ring.empty;
     c.sr = pb_stage_rows(kp / 8);
-    c.col_bytes = pb_col_bytes(kp / 8);
+    c.col_bytes = solve ? pb_solve_col_bytes(kp / 8) : pb_col_bytes(kp / 8);
     c.stage_bytes = kp * c.col_bytes;
     c.nslots = min(PB_MAX_STAGES, PB_RING / c.stage_bytes);
     c.kp = kp;
@@ -806,7 +811,7 @@ __device__ bool gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
     __syncthreads();
     if (!s_skip) {
         const int k = I.k;
-        GramCtx c = ring_ctx(I, chunk, smem, ring);
+        GramCtx c = ring_ctx(I, chunk, smem, ring, false);
         c.out = reinterpret_cast<z64*>(I.scratch + pb_layout(k, I.nchunks).partial) + (size_t)chunk * pb_npairs(k) * 64;
         // Padding columns past k read as zero: no copy writes them.
         if (k < c.kp) {
@@ -884,7 +889,7 @@ __device__ void solve_job(const PbArgs& a, const PbInst& I, int slot, int pass, 
             for (int e = tid; e < n / 2; e += blockDim.x) reinterpret_cast<double2*>(frag)[e] = __ldcg(src + e);
             cached = key;
         }
-        GramCtx c = ring_ctx(I, chunk, smem, ring);
+        GramCtx c = ring_ctx(I, chunk, smem, ring, true);
         if (path == PATH_INVERSE && k <= PB_STAGED_SOLVE_KMAX) {
             fence_proxy_async_all();
             __syncthreads();

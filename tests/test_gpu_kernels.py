@@ -302,6 +302,34 @@ def test_rdiv_upper_reconstructs_to_working_accuracy(fb, backend, oracle):
     fb.kernels.rdiv_upper(backend, Ad, Rd)
     X = Ad.to_host()
     assert np.linalg.norm(X @ R - A) <= 1e-13 * np.linalg.norm(A)
+    # And X is the substitution's result to within what any backward-stable
+    # solve's forward error allows (about cond_1(R) eps).
+    expect = A.copy(order="F")
+    oracle.rdiv_upper(expect, R)
+    cond = np.linalg.norm(R, 1) * np.linalg.norm(np.linalg.inv(R), 1)
+    assert np.linalg.norm(X - expect) <= 1e-15 * cond * np.linalg.norm(expect)
+
+
+@pytest.mark.parametrize("k", [40, 64])
+def test_cholqr2_resident_matches_oracle_at_kappa_1e6(fb, backend, oracle, k):
+    # The C2 conditioning: pass 1's factor is past the product by the inverse,
+    # so the blocked solve runs. R stays within 1e-12 of the oracle's (whose
+    # pass-1 solve is substitution); Q, which Y determines only to about
+    # kappa eps, within that (the measured difference is near 1.3e-11).
+    rng = np.random.default_rng(k + 500)
+    N = 100_000
+    A = conditioned(rng, N, k, 1e6)
+    Qo = A.copy(order="F")
+    Ro, passes_o = oracle.cholqr2(Qo)
+    Y = backend.todevice(A)
+    R = nanbuffer(backend, (k, k))
+    passes, _ = fb.kernels.cholqr2_resident(backend, Y, R)
+    Q, Rh = Y.to_host(), R.to_host()
+    assert passes == passes_o == 2
+    assert np.linalg.norm(Q - Qo) <= 1e6 * 2.0 ** -52 * np.linalg.norm(Qo)
+    assert np.linalg.norm(Rh - Ro) <= 1e-12 * np.linalg.norm(Ro)
+    assert oracle.orthogonality_error(Q) <= 1e-12
+    assert oracle.reconstruction_error(A, Q, Rh) <= 1e-13
 
 
 @pytest.mark.parametrize("k,scale", [(64, 0.01), (37, 0.01), (64, 0.5), (8, 3.0)])

@@ -68,6 +68,13 @@ constexpr int PB_REGION = TR_KMAX * TR_PREP_LD * 16; // one k x k matrix of the 
 // place, so a CTA reuses them across its jobs until it runs a factor step.
 constexpr int PB_RING_OFF = TR_FRAG_DOUBLES * 8;
 constexpr int PB_SMEM = PB_RING_OFF + PB_RING;
+// At k <= 32 the fragments take at most 18 KB, so the ring of that width's
+// Gram and solve jobs starts right after them and takes the rest: five or
+// more slots instead of three or four, which is what their HBM-bound sweeps
+// need in flight. Such a job overwrites the fragment area of wider panels,
+// which the caller then forgets.
+constexpr int PB_SMALL_FRAG_BYTES = 32 * 8 * 9 * 8;
+constexpr int PB_SMALL_RING = PB_SMEM - PB_SMALL_FRAG_BYTES;
 static_assert(2 * PB_REGION <= PB_SMEM, "factor regions exceed shared memory");
 static_assert(PB_WARPS * TR_BUF * 16 <= PB_RING, "transpose buffers exceed the ring");
 
@@ -299,7 +306,7 @@ __device__ void gram_warp(GramCtx& c, uint32_t& full_par) {
     for (int i = 0; i < S::NACC; ++i) acc[i] = 0.0;
     gram_stages<WPG, SR>(c, full_par, h, [&](const unsigned char* base, int q0, int nq) {
         const unsigned char* p = base + lane_off;
-#pragma unroll 2
+#pragma unroll (NB <= 4 ? 4 : 2)
         for (int q = q0; q < nq; q += WPG) gram_kstep<NB, G0>(p + (q >> 2) * 128 + (q & 3) * 16, odelta, flip, acc);
     });
     // The ring is free once every multiplying warp is past its last stage.
@@ -768,14 +775,15 @@ struct PbRing {
 // the instance's width).
 __device__ GramCtx ring_ctx(const PbInst& I, int chunk, unsigned char* smem, const PbRing& ring, bool solve) {
     const int kp = pb_kp(I.k);
+    const bool small = I.k <= PB_STAGED_SOLVE_KMAX;
     GramCtx c;
-    c.ring = smem + PB_RING_OFF;
+    c.ring = smem + (small ? PB_SMALL_FRAG_BYTES : PB_RING_OFF);
     c.full = ring.full;
     c.empty = ring.empty;
     c.sr = pb_stage_rows(kp / 8);
     c.col_bytes = solve ? pb_solve_col_bytes(kp / 8) : pb_col_bytes(kp / 8);
     c.stage_bytes = kp * c.col_bytes;
-    c.nslots = min(PB_MAX_STAGES, PB_RING / c.stage_bytes);
+    c.nslots = min(PB_MAX_STAGES, (small ? PB_SMALL_RING : PB_RING) / c.stage_bytes);
     c.kp = kp;
     c.row0 = (int64_t)chunk * I.chunk_rows;
     c.row1 = min(I.N, c.row0 + I.chunk_rows);
@@ -788,7 +796,8 @@ __device__ GramCtx ring_ctx(const PbInst& I, int chunk, unsigned char* smem, con
 // The Gram chunk `chunk` of pass `pass`: waits (pass >= 2) for the chunk's
 // solve of the previous pass, multiplies unless the instance stopped, adds
 // the arrival, and runs the factor step if it was the last chunk to arrive.
-// Returns whether it ran the factor step (which overwrites the fragments).
+// Returns whether it overwrote cached fragments (a factor step, or a narrow
+// job's ring).
 __device__ bool gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, unsigned char* smem, PbRing& ring,
                          double* red) {
     __shared__ int s_skip, s_bad, s_last;
@@ -846,7 +855,7 @@ __device__ bool gram_job(const PbArgs& a, const PbInst& I, int pass, int chunk, 
         s_last = before == I.nchunks - 1;
     }
     __syncthreads();
-    if (!s_last) return false;
+    if (!s_last) return I.k <= PB_STAGED_SOLVE_KMAX;
     __threadfence();
     factor_step(I, pass, smem, red);
     return true;

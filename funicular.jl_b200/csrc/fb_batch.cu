@@ -22,9 +22,10 @@
 // Gram job: a copy warp streams the chunk through shared memory in stages of
 // about 33 KB (32 rows at k = 64 up to 256 rows at k <= 8) with bulk copies
 // (cp.async.bulk, one per column and stage, no tensor map, so an instance
-// needs no host-encoded descriptor), into a ring of four to six stages
-// guarded by mbarriers. Twelve warps multiply on the FP64 tensor cores (mma m8n8k4 on
-// the real form of the complex product, as the chain's Gram kernel): the
+// needs no host-encoded descriptor), into a ring of four or more stages
+// guarded by mbarriers (135 KB; 190 KB at k <= 32, whose fragments are
+// small). Twelve warps multiply on the FP64 tensor cores (mma m8n8k4 on the
+// real form of the complex product, as the chain's Gram kernel): the
 // upper triangle of 8 x 8 blocks is split into sets of block rows
 // {g, nb-1-g}, which carry equal MMA counts, each set owned by 12, 6, 4 or 3
 // warps that deal out the chunk's k-steps among them; a diagonal block costs
@@ -36,10 +37,10 @@
 // Solve jobs: the product by inv(R), the blocked solve or substitution, as
 // the plan says (the chain's paths, restated for a chunk of rows and the
 // CTA's sixteen warps). Up to k = 32 the product by inv(R) reads its rows
-// through the same ring (15 warps multiply), which keeps 135 KB in flight
-// where one warp's own loads would not; wider panels load straight into
-// registers. Data another CTA wrote during the launch is read
-// through L2 (ld.global.cg), never from a possibly stale L1 line.
+// through the same ring (15 warps multiply), which keeps up to 190 KB in
+// flight where one warp's own loads would not; wider panels load straight
+// into registers. Data another CTA wrote during the launch is read through
+// L2 (ld.global.cg), never from a possibly stale L1 line.
 #include <algorithm>
 #include <memory>
 #include <vector>

@@ -638,24 +638,32 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
     col = 16 * N
     passes = 2  # the third pass runs only after a shift, and the Gram of G X is well conditioned here
     # Host to device and back, per phase: panelmul writes Y (X is generated on
-    # the device); a cholqr2 pass reads Y twice (Gram, solve) and writes it
-    # once; project in two sweeps reads Y, writes Z = G Y, then reads both
-    # (the nested schedule uploads p (p + 1) panels).
+    # the device); cholqr2 reads Y once for the first Gram and once per pass
+    # for the solve, which also takes the next pass's Gram (twice per pass on
+    # a narrowed host tier), and writes it once per pass; project in two
+    # sweeps reads Y, writes Z = G Y, then reads both (the nested schedule
+    # uploads p (p + 1) panels).
     if schedule == "two-sweep":
         up_project, down_project = 3 * col * k, col * k
     elif schedule == "resident":
         up_project, down_project = col * k, 0
     else:
         up_project, down_project = col * sum(widths) + col * p * sum(widths), 0
-    up = {"panelmul": 0, "cholqr2": passes * 2 * col * k, "project": up_project}
+    cholqr2_reads = passes + 1 if fb.panelblas.solves_what_it_stores(Y) else 2 * passes
+    up = {"panelmul": 0, "cholqr2": cholqr2_reads * col * k, "project": up_project}
     down = {"panelmul": col * k, "cholqr2": passes * col * k, "project": down_project}
     Gq = fb.gram(Y)
     orth = float(np.linalg.norm(Gq - np.eye(k)))
     total_ms = sum(ms)
     total_bus = sum(up.values()) + sum(down.values())
-    # The link carries both directions at once: the bound is the slower
-    # direction's bytes over its measured bandwidth.
-    bound_ms = 1e3 * max(sum(up.values()) / (pcie["h2d"] * 1e9), sum(down.values()) / (pcie["d2h"] * 1e9))
+    # The link carries both directions at once: a phase's bound is its slower
+    # direction's bytes over that direction's measured bandwidth. The three
+    # calls run one after another, so the step's bound is the sum over the
+    # phases; the bound if every phase's traffic could overlap every other's
+    # is reported beside it.
+    phase_ms = {ph: 1e3 * max(up[ph] / (pcie["h2d"] * 1e9), down[ph] / (pcie["d2h"] * 1e9)) for ph in up}
+    bound_ms = sum(phase_ms.values())
+    overlapped_ms = 1e3 * max(sum(up.values()) / (pcie["h2d"] * 1e9), sum(down.values()) / (pcie["d2h"] * 1e9))
     out = {"workload": f"streamed range finder, 342^3 Laplacian (N={N}), k={k}, {p} panels of width {max(widths)}, "
                        f"device budget {budget / 1e9:.1f} GB for a {col * k / 1e9:.1f} GB matrix, "
                        f"project schedule {schedule}",
@@ -663,6 +671,9 @@ def run_range_finder(args, fb, backend, torch, device, world, max_over_ranks, ba
            "ms": {"panelmul": ms[0], "cholqr2_streamed": ms[1], "project": ms[2], "step": total_ms},
            "bus_bytes_up": up, "bus_bytes_down": down, "bus_gbs": total_bus / (total_ms * 1e-3) / 1e9,
            "pcie_measured_gbs": pcie, "ms_pcie_bound": bound_ms, "pcie_roofline_frac": bound_ms / total_ms,
+           "ms_pcie_bound_by_phase": phase_ms,
+           "pcie_frac_by_phase": {ph: phase_ms[ph] / v for ph, v in zip(("panelmul", "cholqr2", "project"), ms)},
+           "ms_pcie_bound_phases_overlapped": overlapped_ms,
            "orthogonality_fro": orth, "r_finite": bool(np.isfinite(R).all()), "s_finite": bool(np.isfinite(S).all()),
            "clock": "host wall clock around each synchronous call, the second of two steps"}
     fb.free(Y)

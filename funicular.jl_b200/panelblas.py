@@ -234,41 +234,71 @@ def cholesky_upper(plan, G_dev: DeviceMatrix, N: int, k: int, U_dev: DeviceMatri
     return shifted
 
 
-def rdiv_rows(Y: PanelMatrix, R_dev: DeviceMatrix, *, nbuffers=None) -> PanelMatrix:
-    """rdiv_rows! (src/panelblas.jl:157-169) with the factor already on the device."""
+def gram_rows(Y: PanelMatrix, G_dev: DeviceMatrix, *, nbuffers=None) -> DeviceMatrix:
+    """The Gram sweep of cholqr_pass! (src/panelblas.jl:143): G = Y^H Y
+    accumulated over row blocks, first block overwriting."""
     backend = Y.plan.backend
-    sweep(lambda step, Yb: kernels.rdiv_upper(backend, Yb, R_dev), updatepanels(Y), nbuffers=nbuffers,
-          traversal=rowtraversal(Y))
+    sweep(lambda step, Yb: kernels.gram_accumulate(backend, G_dev, Yb, Yb, 1.0, carry(step)),
+          readpanels(Y), nbuffers=nbuffers, traversal=rowtraversal(Y))
+    return G_dev
+
+
+def rdiv_rows(Y: PanelMatrix, R_dev: DeviceMatrix, *, nbuffers=None, next_gram: DeviceMatrix | None = None) -> PanelMatrix:
+    """rdiv_rows! (src/panelblas.jl:157-169) with the factor already on the
+    device. With next_gram, each solved row block, still on the device, is
+    also accumulated into next_gram as the next pass's Gram sweep would
+    accumulate it after reading the block back: the same blocks in the same
+    order with the same first-step overwrite, so the same bits, one upload
+    sweep fewer."""
+    backend = Y.plan.backend
+
+    def solve(step, Yb):
+        kernels.rdiv_upper(backend, Yb, R_dev)
+        if next_gram is not None:
+            kernels.gram_accumulate(backend, next_gram, Yb, Yb, 1.0, carry(step))
+
+    sweep(solve, updatepanels(Y), nbuffers=nbuffers, traversal=rowtraversal(Y))
     return Y
 
 
-def cholqr_pass(Y: PanelMatrix, nbuffers, U_dev: DeviceMatrix, G_dev: DeviceMatrix, forced_unit_roundoff=None):
-    """cholqr_pass! (src/panelblas.jl:141-146): one pass streamed through row
-    sweeps, the k x k factor staying on the device."""
-    plan = Y.plan
-    backend = plan.backend
-    sweep(lambda step, Yb: kernels.gram_accumulate(backend, G_dev, Yb, Yb, 1.0, carry(step)),
-          readpanels(Y), nbuffers=nbuffers, traversal=rowtraversal(Y))
-    shifted = cholesky_upper(plan, G_dev, Y.N, Y.k, U_dev, forced_unit_roundoff)
-    rdiv_rows(Y, U_dev, nbuffers=nbuffers)
-    return collect_small(U_dev, plan), shifted
+def solves_what_it_stores(Y: PanelMatrix) -> bool:
+    """Whether a row block on the device after the solve holds exactly what
+    the host panels will hold: true unless the host tier narrows (a
+    ComplexF32 tier rounds the block on its way down, and the next pass's
+    Gram is of the rounded values)."""
+    from .panels import host_storage_eltype
+    return np.dtype(host_storage_eltype(Y.plan, Y.dtype)) == np.dtype(Y.dtype)
 
 
 def cholqr2_streamed(Y: PanelMatrix, *, nbuffers=None, forced_unit_roundoff=None) -> np.ndarray:
-    """cholqr2! as the reference runs it (src/panelblas.jl:130-139): two
-    passes, a third when either shifted, every pass two row sweeps. With
-    forced_unit_roundoff the first pass is shifted at once, so all three run:
-    the shifted CholeskyQR3."""
+    """cholqr2! through row sweeps (src/panelblas.jl:130-146): two passes, a
+    third when either of the first two shifted, each pass
+    (cholqr_pass!, src/panelblas.jl:141-146) a Gram, its factor and the
+    solve, the k x k factor staying on the device. The first Gram is its own
+    sweep; a later pass's Gram is taken inside the previous pass's solve
+    sweep when the host tier stores the solved blocks unrounded, else by a
+    sweep of its own as the reference takes it. A pass knows whether another
+    follows once its factor is known, before its solve: a fourth never runs.
+    With forced_unit_roundoff the first pass is shifted at once, so all three
+    run: the shifted CholeskyQR3. When a factor fails, Y holds the previous
+    pass's Q."""
     Y.assert_writable()
     plan = Y.plan
+    fuse = solves_what_it_stores(Y)
     G_dev, U_dev = checkout_device_buffers(plan, Y.dtype, (Y.k, Y.k), 2)
     try:
-        R, s1 = cholqr_pass(Y, nbuffers, U_dev, G_dev, forced_unit_roundoff)
-        R2, s2 = cholqr_pass(Y, nbuffers, U_dev, G_dev)
-        R = R2 @ R
-        if s1 or s2:
-            R3, _ = cholqr_pass(Y, nbuffers, U_dev, G_dev)
-            R = R3 @ R
+        gram_rows(Y, G_dev, nbuffers=nbuffers)
+        R, npasses, p = None, 2, 0
+        while p < npasses:
+            if cholesky_upper(plan, G_dev, Y.N, Y.k, U_dev, forced_unit_roundoff if p == 0 else None):
+                npasses = 3
+            more = p + 1 < npasses
+            rdiv_rows(Y, U_dev, nbuffers=nbuffers, next_gram=G_dev if more and fuse else None)
+            if more and not fuse:
+                gram_rows(Y, G_dev, nbuffers=nbuffers)
+            Rp = collect_small(U_dev, plan)
+            R = Rp if R is None else Rp @ R
+            p += 1
         return R
     finally:
         checkin_device_buffers(plan, [G_dev, U_dev])
@@ -288,7 +318,7 @@ def cholqr2_resident(Y: PanelMatrix, form: str = "fp64", unit_roundoff=None) -> 
     """The backend's cholqr2! when Y fits on the device: every panel goes up
     once, the whole two- or three-pass chain runs on the device
     (kernels.cholqr2_resident), Q comes back down once. Two host-device
-    crossings of the matrix instead of the six of the streamed form. When a
+    crossings of the matrix instead of the five of the streamed form. When a
     Gram matrix stays indefinite the error is raised before anything is
     written back, so Y keeps its values."""
     plan = Y.plan

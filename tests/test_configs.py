@@ -38,7 +38,8 @@ def test_c1_ghost_panels_through_cholqr2_match_the_oracle(fb, backend, oracle, c
     nbytes = C1_N * C1_K * 16
     # resident: the device budget holds the matrix, so cholqr2 runs the device
     # chain; streamed: a budget of about half of it (two staging row blocks of
-    # 2^18 rows), so every pass is two row sweeps, as the reference runs it.
+    # 2^18 rows), so every pass streams through row sweeps: the Gram and the
+    # solve, a later pass's Gram taken inside the previous solve sweep.
     budget = 4 * nbytes if resident else nbytes // 2 + (32 << 20)
     plan = fb.ResidencyPlan(device_budget=budget, host_budget=2 * nbytes + (64 << 20), backend=backend)
     Omega = fb.GhostPanels(np.complex128, C1_N, C1_K, plan=plan, seed=C1_SEED, w=C1_W)

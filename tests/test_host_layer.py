@@ -383,6 +383,39 @@ def test_cholqr2_streamed_matches_the_oracle(fb, oracle, make_plan, rng):
     assert oracle.orthogonality_error(Q) <= orthogonality_bound(N, k)
 
 
+def separate_sweeps(fb, Y, forced_unit_roundoff=None):
+    """cholqr2! with every pass's Gram a sweep of its own, read back from the
+    host panels (the reference's order, src/panelblas.jl:141-146)."""
+    pb, plan = fb.panelblas, Y.plan
+    G = plan.backend.alloc_device(np.complex128, (Y.k, Y.k))
+    U = plan.backend.alloc_device(np.complex128, (Y.k, Y.k))
+    R, npasses, p = None, 2, 0
+    while p < npasses:
+        pb.gram_rows(Y, G)
+        if pb.cholesky_upper(plan, G, Y.N, Y.k, U, forced_unit_roundoff if p == 0 else None):
+            npasses = 3
+        pb.rdiv_rows(Y, U)
+        Rp = pb.collect_small(U, plan)
+        R = Rp if R is None else Rp @ R
+        p += 1
+    return R, npasses
+
+
+@pytest.mark.parametrize("kappa,forced,passes", [(1e5, None, 2), (1e5, 2.0 ** -24, 3), (1e13, None, 3)])
+def test_streamed_gram_taken_in_the_solve_sweep_has_the_bits_of_its_own_sweep(fb, make_plan, rng, kappa, forced,
+                                                                                 passes):
+    N, k, w = 5000, 16, 4
+    A = conditioned(rng, N, k, kappa)
+    plan = make_plan(device_budget=2 * N * w * 16 + 8 * MiB, panel_width=w)
+    Y = fb.PanelMatrix.from_array(A, plan=plan)
+    R = fb.cholqr2(Y, resident=False) if forced is None else fb.cholqr3(Y, resident=False, unit_roundoff=forced)
+    Y2 = fb.PanelMatrix.from_array(A, plan=plan)
+    R2, n = separate_sweeps(fb, Y2, forced)
+    assert n == passes
+    assert np.array_equal(R, R2)
+    assert np.array_equal(Y.to_array(), Y2.to_array())
+
+
 def test_cholqr2_refuses_an_indefinite_gram_and_a_ghost(fb, plan, rng):
     A = randmatrix(rng, 40, 6)
     A[:, 3] = 0

@@ -16,13 +16,19 @@
 // i - kd .. i + 15 + kd, is the MMA A operand (entries of G, loaded once per
 // k-step and reused for every n-tile) against the real form of X as the B
 // operand, each B entry serving both m-tiles. The X rows the CTA's band
-// reaches (256 + 2 kd of them) are staged in shared memory 32 columns at
+// reaches (256 + 2 kd of them) are staged in shared memory 16 columns at
 // a time, column-major with a padded column length so that one fragment load
-// (two rows by four columns) touches 32 distinct banks. A wider band falls
+// (two rows by four columns) touches 32 distinct banks, in two buffers: one
+// CTA an SM copies the next stage with cp.async while its warps multiply
+// the current one, so the tensor pipe does not wait for the copies. Signs
+// of the real form are flipped on the integer pipe, leaving the FP64 pipe,
+// which the MMAs share, to the MMAs. A wider band falls
 // back to the FP64-pipe kernel below: a thread owns one row and CB columns of
 // the output; the blocks of one row tile run side by side over the column
 // chunks, so each diagonal entry comes from DRAM once and from L2 for the
 // other chunks, and the X rows of the band come from L1.
+#include <type_traits>
+
 #include "fb_common.cuh"
 #include "fb_tma.cuh"
 
@@ -73,38 +79,154 @@ constexpr int HBT_MT = 2;                  // 8-row m-tiles a warp owns
 constexpr int HBT_WROWS = 8 * HBT_MT;      // rows a warp owns
 constexpr int HBT_WARPS = 16;
 constexpr int HBT_ROWS = HBT_WARPS * HBT_WROWS;  // rows a CTA owns
-constexpr int HBT_COLS = 32;               // columns of X staged at a time (8 n-tiles)
+constexpr int HBT_COLS = 16;               // columns of X a stage holds
+constexpr int HBT_NT = HBT_COLS / 4;       // n-tiles of a stage
+constexpr int HBT_STAGES = 2;
 constexpr int HBT_KDMAX = 64;
-constexpr int HBT_AHEAD = 2;               // k-steps of band entries loaded ahead (32 products)
 
-// Column length of the staged X tile: HBT_ROWS + 2 kd rows, padded to 2 mod 8 so
-// that the four columns a fragment load reads start 8 banks apart.
-__host__ __device__ inline int hbt_pitch(int kd) {
-    int r = HBT_ROWS + 2 * kd;
-    while ((r & 7) != 2) ++r;
-    return r;
+// Column length of a staged X block: HBT_ROWS + 2 HBT_KDMAX rows (any band
+// up to HBT_KDMAX fits), padded to 2 mod 8 so that the four columns a
+// fragment load reads start 8 banks apart. Fixed, so fragment loads take
+// their column offsets as immediates.
+constexpr int hbt_pitch_for(int rows) { return (rows & 7) == 2 ? rows : hbt_pitch_for(rows + 1); }
+constexpr int HBT_PITCH = hbt_pitch_for(HBT_ROWS + 2 * HBT_KDMAX);
+constexpr size_t HBT_SMEM = (size_t)HBT_STAGES * HBT_PITCH * HBT_COLS * sizeof(z64);
+
+// One 16-byte copy from global to shared memory that completes
+// asynchronously (cp.async, cached in L2 only); src_bytes = 0 reads nothing
+// and writes zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)),
+                 "l"(__cvta_generic_to_global(src)), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
 }
 
-// Part p of G[i][j], zero outside the matrix and the band. The lanes of a
-// warp fall on different sides of the diagonal, so the entry is found without
-// branching: one address (the superdiagonal entry for j >= i, the conjugate
-// of the mirrored one for j < i) and one predicated load.
-__device__ __forceinline__ double band_part(const double* __restrict__ Dg, int64_t lddg, int64_t N, int kd, int64_t i,
-                                            int64_t j, int p) {
-    const int64_t d = j - i;
-    const int64_t ad = d < 0 ? -d : d;
-    const bool live = i < N && j >= 0 && j < N && ad <= kd && !(d == 0 && p);
-    const int64_t at = 2 * ((d >= 0 ? i : j) + ad * lddg) + p;
-    const double v = live ? __ldg(Dg + at) : 0.0;
-    return (d < 0 && p) ? -v : v;
+// x with its sign bit flipped where flip has it set: a negation that takes
+// an integer instruction instead of the FP64 pipe the MMAs run on.
+__device__ __forceinline__ double flip_sign(double x, unsigned flip) {
+    return __hiloint2double(__double2hiint(x) ^ (int)flip, __double2loint(x));
 }
 
+// The A operand of the band product, one lane's entries k-step after
+// k-step. Lane (rr, kr) of m-tile m supplies part p = kr & 1 of G[i][j] with
+// i = wi0 + 8 m + rr and j = j0 + 2 s, j0 = wi0 - kd + (kr >> 1), at k-step s,
+// so its diagonal is d = j - i = dd + 2 s - 8 m, dd = (kr >> 1) - rr - kd,
+// whatever the tile. The entry is Dg[i, d] for d >= 0 and conj(Dg[j, -d])
+// for d < 0: in doubles, base + P_m for d >= 0 and base + Q_m for d < 0, with
+// base = Dg + 2 wi0 and offsets that advance by fixed strides from one k-step
+// to the next (Off = int when every offset a unit reaches fits 32 bits).
+// Which steps are live (the column in the matrix, |d| <= kd, the row in the
+// matrix, not the imaginary part of the main diagonal), where d turns
+// non-negative and where it is zero depend on the lane and m alone, or once
+// per unit on the tile's edges, so a step tests two integer ranges. entry()
+// gives the value as stored; the conjugation (the sign of part 1 where
+// d < 0) is applied by sign() when the entry is used, so nothing waits on a
+// load before the step that multiplies it.
+template <typename Off>
+struct BandFeed {
+    const double* base;
+    Off P[HBT_MT], Q[HBT_MT];
+    Off dP, dQ;
+    int s;                  // k-step of the next entries
+    int L[HBT_MT];          // live steps: L <= s <= L + W, s != Z
+    unsigned W[HBT_MT];
+    int Z[HBT_MT];
+    int S[HBT_MT];          // first step with d >= 0
+    int T[HBT_MT];          // steps below T take a flipped sign (S for part 1, none for part 0)
+
+    __device__ __forceinline__ void start(const double* __restrict__ Dg, int64_t wi0, int rr, int kr, int kd,
+                                          int64_t N, int64_t lddg) {
+        const int p = kr & 1;
+        const int dd = (kr >> 1) - rr - kd;
+        const int64_t j0 = wi0 - kd + (kr >> 1);
+        base = Dg + 2 * wi0;
+        dP = (Off)(4 * lddg);
+        dQ = (Off)(4 - 4 * lddg);
+        s = 0;
+        // The column j0 + 2 s lies in the matrix for first <= s <= last.
+        const int64_t first = j0 >= 0 ? 0 : (1 - j0) >> 1;
+        const int64_t last64 = (N - 1 - j0) >> 1;
+        const int lo = (int)(first < 4096 ? first : 4096);
+        const int hi = (int)(last64 < 4096 ? (last64 < -1 ? -1 : last64) : 4096);
+        constexpr int NEVER = 1 << 30;
+#pragma unroll
+        for (int m = 0; m < HBT_MT; ++m) {
+            const int e = 8 * m - dd;   // d = 2 s - e
+            P[m] = (Off)(2 * (8 * m + rr) + p - 2 * lddg * e);
+            Q[m] = (Off)(2 * (j0 - wi0) + p + 2 * lddg * e);
+            S[m] = (e + 1) >> 1;
+            T[m] = p ? S[m] : -NEVER;
+            Z[m] = (p && !(e & 1)) ? e >> 1 : -NEVER;
+            const int sa = (e - kd + 1) >> 1, sb = (e + kd) >> 1;   // |2 s - e| <= kd
+            const int l = sa > lo ? sa : lo, h = sb < hi ? sb : hi;
+            const bool any = h >= l && wi0 + 8 * m + rr < N;
+            L[m] = any ? l : NEVER;
+            W[m] = any ? (unsigned)(h - l) : 0u;
+        }
+    }
+    // Part p of m-tile m's entry at step s, as stored.
+    __device__ __forceinline__ double entry(int m) const {
+        const bool live = (unsigned)(s - L[m]) <= W[m] && s != Z[m];
+        const Off at = s < S[m] ? Q[m] : P[m];
+        return live ? __ldg(base + at) : 0.0;
+    }
+    // The sign flip that turns m-tile m's stored entry at step st into G's.
+    __device__ __forceinline__ unsigned sign(int st, int m) const { return st < T[m] ? 0x80000000u : 0u; }
+    __device__ __forceinline__ void advance() {
+#pragma unroll
+        for (int m = 0; m < HBT_MT; ++m) {
+            P[m] += dP;
+            Q[m] += dQ;
+        }
+        ++s;
+    }
+};
+
+// Whether every offset BandFeed<int> forms stays in 32 bits: |offset| is at
+// most 2 lddg (kd + 24) + 2 (kd + 40) over the steps a unit reaches.
+__host__ __device__ inline bool hbt_offsets_fit_int(int64_t lddg, int kd) {
+    return 2 * lddg * (int64_t)(kd + 32) + 4096 < ((int64_t)1 << 31);
+}
+
+// Copies rows xrow0 .. xrow0 + staged - 1 of columns c0 .. c0 + HBT_COLS - 1
+// of X into a stage buffer (column-major, HBT_PITCH rows a column), zeros for
+// rows outside the matrix and columns past `cols`.
+__device__ __forceinline__ void hbt_stage(z64* __restrict__ xs, int staged, const z64* __restrict__ X,
+                                          int64_t ldx, int64_t N, int cols, int64_t xrow0, int c0) {
+#pragma unroll 1
+    for (int c = 0; c < HBT_COLS; ++c) {
+        const bool col_live = c0 + c < cols;
+        const z64* column = X + (int64_t)(col_live ? c0 + c : 0) * ldx;
+        for (int r = threadIdx.x; r < staged; r += blockDim.x) {
+            const int64_t gr = xrow0 + r;
+            const bool live = col_live && gr >= 0 && gr < N;
+            cp_async16(xs + c * HBT_PITCH + r, live ? column + gr : X, live ? 16 : 0);
+        }
+    }
+}
+
+// One CTA an SM walks units (a tile of HBT_ROWS rows, a stage of HBT_COLS
+// columns), the tile's columns in order, then its next tile. The X rows the
+// next unit reaches are copied into the other stage buffer while this unit's
+// MMAs run. A warp's window of k-steps (2 kd + 16 columns) is the union of its
+// two m-tiles' bands: m-tile m's rows 8 m .. 8 m + 7 reach k-steps
+// 4 m .. 4 m + kd + 3, so the window runs in three phases (m-tile 0 alone,
+// both, m-tile 1 alone), each a straight loop, and no MMA multiplies a
+// k-step outside its m-tile's band.
+template <typename Off>
 __global__ void __launch_bounds__(HBT_WARPS * 32, 1)
 hband_dmma_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, int64_t ldx,
                   const z64* __restrict__ Dg, int64_t lddg, int64_t N, int kd, int cols) {
+    static_assert(HBT_MT == 2, "the phases below are written for two m-tiles a warp");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    z64* xs = reinterpret_cast<z64*>(smem_raw);   // HBT_COLS columns of `pitch` rows
-    const int pitch = hbt_pitch(kd);
+    z64* xs0 = reinterpret_cast<z64*>(smem_raw);   // HBT_STAGES buffers of HBT_COLS columns of HBT_PITCH rows
+    constexpr int pitch = HBT_PITCH;
+    constexpr int stage_elems = HBT_PITCH * HBT_COLS;
     const int staged = HBT_ROWS + 2 * kd;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rr = lane >> 2, kr = lane & 3, nr = lane >> 2;
@@ -112,85 +234,90 @@ hband_dmma_kernel(z64* __restrict__ Y, int64_t ldy, const z64* __restrict__ X, i
     // The B entry this lane supplies: part (p ^ o) of X[row][col], negated
     // for (p, o) = (1, 0): the real form of the complex product.
     const int bpart = p ^ o;
-    const double bsign = (p == 1 && o == 0) ? -1.0 : 1.0;
-    const int nsteps = kd + HBT_WROWS / 2;         // k-steps of a warp's band: 2 kd + 16 columns
+    const unsigned bflip = (p == 1 && o == 0) ? 0x80000000u : 0u;
     const int64_t tiles = (N + HBT_ROWS - 1) / HBT_ROWS;
-    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int64_t i0 = tile * HBT_ROWS;
-        const int64_t xrow0 = i0 - kd;             // first staged row (may be negative: zeros)
-        const int64_t wi0 = i0 + HBT_WROWS * warp; // this warp's first row
-        for (int c0 = 0; c0 < cols; c0 += HBT_COLS) {
-            __syncthreads();   // the previous chunk's fragments have all been read
-            for (int e = threadIdx.x; e < staged * HBT_COLS; e += blockDim.x) {
-                const int r = e % staged, c = e / staged;
-                const int64_t gr = xrow0 + r;
-                z64 v = zmake(0.0, 0.0);
-                if (gr >= 0 && gr < N && c0 + c < cols) v = X[gr + (int64_t)(c0 + c) * ldx];
-                xs[c * pitch + r] = v;
-            }
-            __syncthreads();
-            double acc[HBT_MT][8][2];
+    const int nchunks = (cols + HBT_COLS - 1) / HBT_COLS;
+    const int64_t mine = (int64_t)blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t units = mine * nchunks;
+    auto unit_row0 = [&](int64_t u) { return ((int64_t)blockIdx.x + (u / nchunks) * gridDim.x) * HBT_ROWS; };
+    auto unit_col0 = [&](int64_t u) { return (int)(u % nchunks) * HBT_COLS; };
+    const double* dg = reinterpret_cast<const double*>(Dg);
+
+    if (units > 0) hbt_stage(xs0, staged, X, ldx, N, cols, unit_row0(0) - kd, unit_col0(0));
+    cp_async_commit();
+    for (int64_t u = 0; u < units; ++u) {
+        const int64_t i0 = unit_row0(u);
+        const int c0 = unit_col0(u);
+        const int64_t wi0 = i0 + HBT_WROWS * warp;   // this warp's first row
+        BandFeed<Off> feed;
+        feed.start(dg, wi0, rr, kr, kd, N, lddg);
+        // The band entries of k-steps s and s + 1 (the next two to multiply);
+        // the first two do not depend on the stage, so they load across the
+        // wait.
+        double e0[HBT_MT], e1[HBT_MT];
 #pragma unroll
-            for (int m = 0; m < HBT_MT; ++m)
+        for (int m = 0; m < HBT_MT; ++m) e0[m] = feed.entry(m);
+        feed.advance();
 #pragma unroll
-                for (int t = 0; t < 8; ++t) acc[m][t][0] = acc[m][t][1] = 0.0;
-            if (wi0 < N) {
-                // k-step s covers columns jb, jb + 1 with jb = wi0 - kd + 2 s
-                // (the union of the m-tiles' bands); this lane's A entry of
-                // m-tile m is G[wi0 + 8 m + rr][jb + (kr >> 1)], part p. The
-                // entries of the next HBT_AHEAD steps are in flight.
-                const double* dg = reinterpret_cast<const double*>(Dg);
-                const int64_t j0 = wi0 - kd + (kr >> 1);
-                double ring[HBT_MT][HBT_AHEAD];
+        for (int m = 0; m < HBT_MT; ++m) e1[m] = feed.entry(m);
+        feed.advance();
+        // One barrier a unit: past it, unit u's copies (the only group in
+        // flight) are visible to every warp, and every warp has finished
+        // unit u - 1, so unit u + 1 may land in the buffer that unit read.
+        cp_async_wait<0>();
+        __syncthreads();
+        if (u + 1 < units) {
+            hbt_stage(xs0 + ((u + 1) & 1) * stage_elems, staged, X, ldx, N, cols, unit_row0(u + 1) - kd,
+                      unit_col0(u + 1));
+            cp_async_commit();
+        }
+        const z64* xs = xs0 + (u & 1) * stage_elems;
+        double acc[HBT_MT][HBT_NT][2];
 #pragma unroll
-                for (int m = 0; m < HBT_MT; ++m)
+        for (int m = 0; m < HBT_MT; ++m)
 #pragma unroll
-                    for (int q = 0; q < HBT_AHEAD; ++q)
-                        ring[m][q] = band_part(dg, lddg, N, kd, wi0 + 8 * m + rr, j0 + 2 * q, p);
-                // One k-step against the eight n-tiles: B is rows jb + (kr >> 1)
-                // of the staged tile, columns 4 t + (nr >> 1); each B entry
-                // serves every m-tile.
-                auto step = [&](int st, const double (&a)[HBT_MT]) {
-                    const int lr = (int)(wi0 - xrow0) - kd + 2 * st + (kr >> 1);
-                    const double* xb = reinterpret_cast<const double*>(xs + (nr >> 1) * pitch + lr) + bpart;
+            for (int t = 0; t < HBT_NT; ++t) acc[m][t][0] = acc[m][t][1] = 0.0;
+        if (wi0 < N) {
+            // k-steps [sb, se) with m-tiles MLO..MHI multiplying: B is local
+            // rows HBT_WROWS warp + 2 s + (kr >> 1) of the stage, columns
+            // 4 t + (nr >> 1), each B entry serving every multiplying m-tile;
+            // the entries of step s + 2 load while step s multiplies.
+            const double* xb0 = reinterpret_cast<const double*>(xs + (nr >> 1) * pitch + HBT_WROWS * warp + (kr >> 1)) +
+                                bpart;
+            auto phase = [&](auto mlo, auto mhi, int sb, int se) {
+                constexpr int MLO = decltype(mlo)::value, MHI = decltype(mhi)::value;
+#pragma unroll 2
+                for (int s = sb; s < se; ++s) {
+                    double a[HBT_MT];
 #pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const double b = bsign * xb[2 * (4 * t) * pitch];
-#pragma unroll
-                        for (int m = 0; m < HBT_MT; ++m) dmma_884(acc[m][t][0], acc[m][t][1], a[m], b);
+                    for (int m = 0; m < HBT_MT; ++m) {
+                        a[m] = flip_sign(e0[m], feed.sign(s, m));
+                        e0[m] = e1[m];
+                        e1[m] = feed.entry(m);
                     }
-                };
-                int s = 0;
-                for (; s + HBT_AHEAD <= nsteps; s += HBT_AHEAD) {
+                    feed.advance();
+                    const double* xb = xb0 + 4 * s;
+                    double b[HBT_NT];
 #pragma unroll
-                    for (int q = 0; q < HBT_AHEAD; ++q) {
-                        double a[HBT_MT];
+                    for (int t = 0; t < HBT_NT; ++t) b[t] = flip_sign(xb[2 * (4 * t) * pitch], bflip);
 #pragma unroll
-                        for (int m = 0; m < HBT_MT; ++m) {
-                            a[m] = ring[m][q];
-                            ring[m][q] = band_part(dg, lddg, N, kd, wi0 + 8 * m + rr, j0 + 2 * (s + q + HBT_AHEAD), p);
-                        }
-                        step(s + q, a);
-                    }
+                    for (int m = MLO; m <= MHI; ++m)
+#pragma unroll
+                        for (int t = 0; t < HBT_NT; ++t) dmma_884(acc[m][t][0], acc[m][t][1], a[m], b[t]);
                 }
+            };
+            phase(std::integral_constant<int, 0>(), std::integral_constant<int, 0>(), 0, 4);
+            phase(std::integral_constant<int, 0>(), std::integral_constant<int, 1>(), 4, kd + 4);
+            phase(std::integral_constant<int, 1>(), std::integral_constant<int, 1>(), kd + 4, kd + 8);
+        }
 #pragma unroll
-                for (int q = 0; q < HBT_AHEAD; ++q)
-                    if (s + q < nsteps) {
-                        double a[HBT_MT];
+        for (int m = 0; m < HBT_MT; ++m) {
+            const int64_t row = wi0 + 8 * m + rr;
+            if (row >= N) continue;
 #pragma unroll
-                        for (int m = 0; m < HBT_MT; ++m) a[m] = ring[m][q];
-                        step(s + q, a);
-                    }
-            }
-#pragma unroll
-            for (int m = 0; m < HBT_MT; ++m) {
-                const int64_t row = wi0 + 8 * m + rr;
-                if (row >= N) continue;
-#pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const int col = c0 + 4 * t + cq;
-                    if (col < cols) Y[row + (int64_t)col * ldy] = zmake(acc[m][t][0], acc[m][t][1]);
-                }
+            for (int t = 0; t < HBT_NT; ++t) {
+                const int col = c0 + 4 * t + cq;
+                if (col < cols) Y[row + (int64_t)col * ldy] = zmake(acc[m][t][0], acc[m][t][1]);
             }
         }
     }
@@ -227,13 +354,14 @@ int fb_zhband_apply(fb_z128* Y, int64_t ldy, const fb_z128* X, int64_t ldx, cons
         return FB_EINVAL;
     }
     if (kd <= HBT_KDMAX) {
-        const size_t smem = (size_t)hbt_pitch(kd) * HBT_COLS * sizeof(z64);
-        FB_CUDA(cudaFuncSetAttribute(hband_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        const bool narrow = hbt_offsets_fit_int(lddg, kd);
+        auto kernel = narrow ? hband_dmma_kernel<int> : hband_dmma_kernel<int64_t>;
+        FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HBT_SMEM),
                 "cudaFuncSetAttribute(hband_dmma_kernel)");
         const int64_t tiles = (N + HBT_ROWS - 1) / HBT_ROWS;
-        int64_t grid = (int64_t)sm_count() * 4;
+        int64_t grid = (int64_t)sm_count();   // one CTA an SM (its shared memory), each walking its tiles
         if (grid > tiles) grid = tiles;
-        hband_dmma_kernel<<<(unsigned)grid, HBT_WARPS * 32, smem, stream_of(queue)>>>(
+        kernel<<<(unsigned)grid, HBT_WARPS * 32, HBT_SMEM, stream_of(queue)>>>(
             reinterpret_cast<z64*>(Y), ldy, reinterpret_cast<const z64*>(X), ldx, reinterpret_cast<const z64*>(Dg),
             lddg, N, kd, cols);
         FB_LAUNCHED("hband_dmma_kernel");

@@ -124,7 +124,10 @@ def test_project_adjoint_matches_the_oracle(fb, backend, oracle, hermitian, k):
     assert rel(Qbar.to_host(), base + ref) < 1e-13
 
 
-@pytest.mark.parametrize("N,kd,cols", [(1000, 5, 3), (50, 64, 7), (4096, 0, 4), (20000, 64, 9)])
+# The last two walk several row tiles a CTA (one CTA an SM, 256 rows a tile),
+# with partial column stages and a ragged last tile.
+@pytest.mark.parametrize("N,kd,cols", [(1000, 5, 3), (50, 64, 7), (4096, 0, 4), (20000, 64, 9), (200_003, 64, 20),
+                                       (90_001, 17, 33)])
 def test_hermitian_band_apply_matches_the_oracle(fb, backend, oracle, N, kd, cols):
     rng = np.random.default_rng(N + kd)
     Dg = randmatrix(rng, N, kd + 1)
@@ -132,6 +135,22 @@ def test_hermitian_band_apply_matches_the_oracle(fb, backend, oracle, N, kd, col
     G = fb.HermitianBand(backend, Dg)
     Y = backend.alloc_device(np.complex128, (N, cols))
     G.apply(backend, Y, backend.todevice(X))
+    backend.sync_all()
+    assert rel(Y.to_host(), oracle.hermitian_band(Dg) @ X) < 1e-14
+
+
+def test_hermitian_band_apply_with_a_wide_band_stride(fb, backend, oracle):
+    # Dg's columns 2^25 entries apart: the kernel's band offsets no longer fit
+    # 32 bits and it forms them in 64.
+    rng = np.random.default_rng(77)
+    N, kd, cols, ld = 3001, 2, 5, 1 << 25
+    Dg = randmatrix(rng, N, kd + 1)
+    store = backend.alloc_device(np.complex128, (ld, kd + 1))
+    view = store.view(slice(0, N), slice(None))
+    backend.h2d(view, Dg)
+    X = randmatrix(rng, N, cols)
+    Y = backend.alloc_device(np.complex128, (N, cols))
+    fb.kernels.hband_apply(backend, Y, backend.todevice(X), view)
     backend.sync_all()
     assert rel(Y.to_host(), oracle.hermitian_band(Dg) @ X) < 1e-14
 
